@@ -1,0 +1,686 @@
+// libhfg host runtime: context creation (shells, shell pairs, primitive
+// pairs, Schwarz bounds on the device), J/K launch plans, and the C-ABI
+// entry points declared in include/hfg.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "boys.cuh"
+#include "hfg_ctx.h"
+#include "jk_dispatch.h"
+
+using namespace hfg;
+
+namespace hfg {
+
+int set_error(hfg_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int cuda_check(hfg_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return HFG_OK;
+  const int code = (e == cudaErrorMemoryAllocation) ? HFG_ERR_OOM : HFG_ERR_CUDA;
+  return set_error(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define HFG_CUDA(ctx, call)                               \
+  do {                                                    \
+    int _rc = cuda_check((ctx), (call), #call);           \
+    if (_rc != HFG_OK) return _rc;                        \
+  } while (0)
+
+// McMurchie-Davidson flop count per primitive quartet of each class, from
+// hf-rs's loops (src/shell_integrals.rs:101-131, src/integrals.rs:70-101,
+// 259-346, 905-971); the work unit of the roofline.
+static double wmd_flops(int la, int lb, int lc, int ld) {
+  static const std::map<std::tuple<int, int, int, int>, double> t = {
+      {{0, 0, 0, 0}, 61},     {{1, 0, 0, 0}, 126},    {{1, 0, 1, 0}, 333},    {{1, 1, 0, 0}, 327},
+      {{1, 1, 1, 0}, 1072},   {{1, 1, 1, 1}, 3916},   {{2, 0, 0, 0}, 256},    {{2, 0, 1, 0}, 771},
+      {{2, 0, 1, 1}, 2683},   {{2, 0, 2, 0}, 1872},   {{2, 1, 0, 0}, 747},    {{2, 1, 1, 0}, 2647},
+      {{2, 1, 1, 1}, 9994},   {{2, 1, 2, 0}, 6751},   {{2, 1, 2, 1}, 25570},  {{2, 2, 0, 0}, 1776},
+      {{2, 2, 1, 0}, 6607},   {{2, 2, 1, 1}, 25354},  {{2, 2, 2, 0}, 16978},  {{2, 2, 2, 1}, 64681},
+      {{2, 2, 2, 2}, 162643}};
+  auto it = t.find({la, lb, lc, ld});
+  return it == t.end() ? 0.0 : it->second;
+}
+
+// Boys grid values F_0..F_{kBoysCols-1} at T = idx * 0.05, by the series at
+// the highest tabulated order (47) and downward recursion, as hf-rs builds
+// its table (src/integrals.rs:27-57).
+static const std::vector<double>& boys_table_host() {
+  static std::vector<double> table;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    const int M = 47;
+    table.assign((size_t)kBoysRows * kBoysCols, 0.0);
+    std::vector<double> row(M + 1);
+    for (int idx = 0; idx < kBoysRows; ++idx) {
+      const double t = idx * kBoysStep;
+      const double et = std::exp(-t);
+      double term = 1.0 / (2 * M + 1), sum = term;
+      for (long i = 1; i <= 10000; ++i) {
+        term *= 2.0 * t / (double)(2 * M + 2 * i + 1);
+        sum += term;
+        if (term < sum * 1e-17) break;
+      }
+      row[M] = et * sum;
+      for (int m = M - 1; m >= 0; --m) row[m] = (2.0 * t * row[m + 1] + et) / (2 * m + 1);
+      for (int m = 0; m < kBoysCols; ++m) table[(size_t)idx * kBoysCols + m] = row[m];
+    }
+  });
+  return table;
+}
+
+static int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+// hf-rs Cartesian component order (src/basis.rs:418-445, :179-188).
+static void cart_order(int l, std::vector<std::array<int, 3>>& out) {
+  out.clear();
+  if (l == 2) {
+    out = {{2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+    return;
+  }
+  for (int lx = l; lx >= 0; --lx)
+    for (int ly = l - lx; ly >= 0; --ly) out.push_back({lx, ly, l - lx - ly});
+}
+
+static double dfact(int n) {  // (n)!! with n <= 0 -> 1
+  double r = 1.0;
+  for (int k = n; k > 0; k -= 2) r *= k;
+  return r;
+}
+
+static double comp_scale_host(const std::array<int, 3>& l) {
+  return 1.0 / std::sqrt(dfact(2 * l[0] - 1) * dfact(2 * l[1] - 1) * dfact(2 * l[2] - 1));
+}
+
+// Groups the Cartesian functions into shells with the semantics of hf-rs's
+// shell_ranges (src/ao.rs:133-164) and recovers the shell contraction
+// coefficients (component coefficient / component scale).
+static int build_shells(hfg_ctx* ctx, const hfg_basis* b) {
+  if (!b || b->n <= 0 || !b->center || !b->lxyz || !b->atom || !b->prim_off || !b->exps || !b->coefs)
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "empty or incomplete basis description");
+  const int n = b->n;
+  ctx->n = n;
+  std::vector<std::array<int, 3>> order;
+  int start = 0;
+  while (start < n) {
+    const int* l0 = b->lxyz + 3 * start;
+    const int l = l0[0] + l0[1] + l0[2];
+    if (l < 0 || l > 7) return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid angular momentum");
+    if (l > kLMax) return set_error(ctx, HFG_ERR_UNSUPPORTED, "angular momentum above d is not built into the kernels");
+    const int cnt = ncart(l);
+    if (start + cnt > n) return set_error(ctx, HFG_ERR_INVALID_INPUT, "incomplete Cartesian shell");
+    const int K = b->prim_off[start + 1] - b->prim_off[start];
+    if (K <= 0) return set_error(ctx, HFG_ERR_INVALID_INPUT, "function without primitives");
+    cart_order(l, order);
+    Shell sh{};
+    for (int k = 0; k < 3; ++k) {
+      sh.c[k] = b->center[3 * start + k];
+      if (!std::isfinite(sh.c[k])) return set_error(ctx, HFG_ERR_INVALID_INPUT, "non-finite geometry");
+    }
+    sh.l = l;
+    sh.K = K;
+    sh.ao = start;
+    sh.atom = b->atom[start];
+    sh.prim_off = (int)ctx->exps.size();
+    const int p0 = b->prim_off[start];
+    const double s0 = comp_scale_host(order[0]);
+    for (int q = 0; q < K; ++q) {
+      const double e = b->exps[p0 + q], c = b->coefs[p0 + q];
+      if (!(e > 0.0) || !std::isfinite(e) || !std::isfinite(c))
+        return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid primitive");
+      ctx->exps.push_back(e);
+      ctx->coefs.push_back(c / s0);
+    }
+    for (int f = 0; f < cnt; ++f) {
+      const int g = start + f;
+      const int* lg = b->lxyz + 3 * g;
+      if (lg[0] != order[f][0] || lg[1] != order[f][1] || lg[2] != order[f][2])
+        return set_error(ctx, HFG_ERR_UNSUPPORTED, "Cartesian components not in hf-rs build_basis order");
+      if (b->atom[g] != sh.atom || b->prim_off[g + 1] - b->prim_off[g] != K)
+        return set_error(ctx, HFG_ERR_INVALID_INPUT, "noncontiguous or incomplete Cartesian shell");
+      for (int k = 0; k < 3; ++k)
+        if (b->center[3 * g + k] != sh.c[k])
+          return set_error(ctx, HFG_ERR_INVALID_INPUT, "noncontiguous or incomplete Cartesian shell");
+      const double sg = comp_scale_host(order[f]);
+      for (int q = 0; q < K; ++q) {
+        if (b->exps[b->prim_off[g] + q] != ctx->exps[sh.prim_off + q])
+          return set_error(ctx, HFG_ERR_INVALID_INPUT, "noncontiguous or incomplete Cartesian shell");
+        const double c = b->coefs[b->prim_off[g] + q] / sg;
+        const double ref = ctx->coefs[sh.prim_off + q];
+        if (std::fabs(c - ref) > 1e-12 * std::max(1.0, std::fabs(ref)))
+          return set_error(ctx, HFG_ERR_UNSUPPORTED, "component coefficients do not share one contraction");
+      }
+    }
+    ctx->shells.push_back(sh);
+    start += cnt;
+  }
+  return HFG_OK;
+}
+
+// Oriented pair (la >= lb, Ka >= Kb on ties) with its primitive pairs.
+static void make_pair(const hfg_ctx* ctx, int a, int b, PairInfo& pi, std::vector<PrimPair>& pp, int owner) {
+  const Shell& A = ctx->shells[a];
+  const Shell& B = ctx->shells[b];
+  pi.Ax = A.c[0];
+  pi.Ay = A.c[1];
+  pi.Az = A.c[2];
+  pi.ABx = A.c[0] - B.c[0];
+  pi.ABy = A.c[1] - B.c[1];
+  pi.ABz = A.c[2] - B.c[2];
+  pi.ao_a = A.ao;
+  pi.ao_b = B.ao;
+  pi.same = (a == b);
+  pi.pp_off = (int)pp.size();
+  pi.npp = A.K * B.K;
+  const double ab2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
+  for (int i = 0; i < A.K; ++i)
+    for (int j = 0; j < B.K; ++j) {
+      const double al = ctx->exps[A.prim_off + i], be = ctx->exps[B.prim_off + j];
+      const double p = al + be, inv_p = 1.0 / p;
+      PrimPair q{};
+      q.p = p;
+      q.inv_p = inv_p;
+      // P - A = beta (B - A) / p
+      q.PAx = -be * pi.ABx * inv_p;
+      q.PAy = -be * pi.ABy * inv_p;
+      q.PAz = -be * pi.ABz * inv_p;
+      q.kp = ctx->coefs[A.prim_off + i] * ctx->coefs[B.prim_off + j] * std::exp(-al * be * inv_p * ab2) * inv_p;
+      q.bound = 0.0;
+      q.pad = (double)owner;
+      pp.push_back(q);
+    }
+}
+
+static bool oriented_swap(const Shell& A, const Shell& B) { return A.l < B.l || (A.l == B.l && A.K < B.K); }
+
+static int build_pairs(hfg_ctx* ctx) {
+  const int ns = (int)ctx->shells.size();
+  ctx->ref_pairs.clear();
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b <= a; ++b) ctx->ref_pairs.push_back({a, b});
+  const long np = (long)ctx->ref_pairs.size();
+  // class of each oriented pair
+  std::map<std::tuple<int, int, int, int>, std::vector<long>> by_class;
+  for (long r = 0; r < np; ++r) {
+    auto [a, b] = ctx->ref_pairs[r];
+    if (oriented_swap(ctx->shells[a], ctx->shells[b])) std::swap(a, b);
+    by_class[{ctx->shells[a].l, ctx->shells[b].l, ctx->shells[a].K, ctx->shells[b].K}].push_back(r);
+  }
+  // grouped (unsorted) tables for the bound computation
+  std::vector<PairInfo> gp;
+  std::vector<PrimPair> gprim;
+  std::vector<long> grouped_ref;
+  std::vector<PairClass> cls;
+  for (auto& [key, refs] : by_class) {
+    PairClass c{std::get<0>(key), std::get<1>(key), std::get<2>(key), std::get<3>(key), (int)gp.size(),
+                (int)refs.size()};
+    for (long r : refs) {
+      auto [a, b] = ctx->ref_pairs[r];
+      if (oriented_swap(ctx->shells[a], ctx->shells[b])) std::swap(a, b);
+      PairInfo pi{};
+      make_pair(ctx, a, b, pi, gprim, (int)gp.size());
+      pi.cls = (int)cls.size();
+      gp.push_back(pi);
+      grouped_ref.push_back(r);
+    }
+    cls.push_back(c);
+  }
+  // device bounds
+  HFG_CUDA(ctx, ctx->d_pairs.alloc(gp.size()));
+  HFG_CUDA(ctx, ctx->d_prims.alloc(gprim.size()));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_pairs.p, gp.data(), gp.size() * sizeof(PairInfo), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_prims.p, gprim.data(), gprim.size() * sizeof(PrimPair),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  DevBuf<double> dq, dpb;
+  HFG_CUDA(ctx, dq.alloc(gp.size()));
+  HFG_CUDA(ctx, dpb.alloc(gprim.size()));
+  for (const auto& c : cls) {
+    HFG_CUDA(ctx, launch_schwarz(c.la, c.lb, ctx->d_pairs.p, ctx->d_prims.p, c.first, c.count, ctx->d_boys64.p,
+                                 dq.p + c.first, 0, ctx->stream));
+    const int p0 = gp[c.first].pp_off;
+    const int p1 = gp[c.first + c.count - 1].pp_off + gp[c.first + c.count - 1].npp;
+    HFG_CUDA(ctx, launch_schwarz(c.la, c.lb, ctx->d_pairs.p, ctx->d_prims.p, p0, p1 - p0, ctx->d_boys64.p,
+                                 dpb.p + p0, 1, ctx->stream));
+  }
+  std::vector<double> Q(gp.size()), PB(gprim.size());
+  HFG_CUDA(ctx, cudaMemcpyAsync(Q.data(), dq.p, Q.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(PB.data(), dpb.p, PB.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  dq.release();
+  dpb.release();
+  for (size_t i = 0; i < gprim.size(); ++i) gprim[i].bound = PB[i];
+  // sort each class by Q descending (ties: hf-rs order), primitives by bound
+  ctx->h_pairs.clear();
+  ctx->h_prims.clear();
+  ctx->sorted_Q.clear();
+  ctx->ref_to_sorted.assign(np, -1);
+  ctx->classes = cls;
+  for (auto& c : ctx->classes) {
+    std::vector<int> idx(c.count);
+    std::iota(idx.begin(), idx.end(), c.first);
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return Q[x] > Q[y]; });
+    c.first = (int)ctx->h_pairs.size();
+    for (int g : idx) {
+      PairInfo pi = gp[g];
+      std::vector<PrimPair> pr(gprim.begin() + pi.pp_off, gprim.begin() + pi.pp_off + pi.npp);
+      std::stable_sort(pr.begin(), pr.end(), [](const PrimPair& x, const PrimPair& y) { return x.bound > y.bound; });
+      pi.pp_off = (int)ctx->h_prims.size();
+      for (auto& q : pr) {
+        q.pad = (double)ctx->h_pairs.size();
+        ctx->h_prims.push_back(q);
+      }
+      ctx->ref_to_sorted[grouped_ref[g]] = (int)ctx->h_pairs.size();
+      ctx->h_pairs.push_back(pi);
+      ctx->sorted_Q.push_back(Q[g]);
+    }
+  }
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_pairs.p, ctx->h_pairs.data(), ctx->h_pairs.size() * sizeof(PairInfo),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_prims.p, ctx->h_prims.data(), ctx->h_prims.size() * sizeof(PrimPair),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return HFG_OK;
+}
+
+// Launch plan for (Schwarz threshold, FP32 threshold, precision): for every
+// pair of pair classes (bra class >= ket class) and every bra pair, the
+// significant kets form a prefix of the ket class (kets sorted by Q); in
+// mixed precision the kets below the FP32 threshold form the tail of it.
+static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, int precision, Plan*& out) {
+  auto key = std::make_tuple(thr, precision == HFG_MIXED ? mixed : 0.0, prim_eps, precision);
+  auto it = ctx->plans.find(key);
+  if (it != ctx->plans.end()) {
+    out = it->second.get();
+    return HFG_OK;
+  }
+  auto plan = std::make_unique<Plan>();
+  std::map<std::tuple<int, int, int, int, int, int>, int> lidx;
+  auto get_launch = [&](int la, int lb, int lc, int ld, int G, bool fp32) -> Launch& {
+    auto k = std::make_tuple(la, lb, lc, ld, G, (int)fp32);
+    auto f = lidx.find(k);
+    if (f != lidx.end()) return plan->launches[f->second];
+    lidx[k] = (int)plan->launches.size();
+    Launch L;
+    L.la = la;
+    L.lb = lb;
+    L.lc = lc;
+    L.ld = ld;
+    L.G = G;
+    L.fp32 = fp32;
+    L.prefix.push_back(0);
+    plan->launches.push_back(std::move(L));
+    return plan->launches.back();
+  };
+  const auto& Q = ctx->sorted_Q;
+  // cumulative primitive-pair counts for the nominal primitive-quartet totals
+  std::vector<double> cum(ctx->h_pairs.size() + 1, 0.0);
+  for (size_t i = 0; i < ctx->h_pairs.size(); ++i) cum[i + 1] = cum[i] + ctx->h_pairs[i].npp;
+  hfg_jk_stats st{};
+  const int nc = (int)ctx->classes.size();
+  for (int cb = 0; cb < nc; ++cb) {
+    const PairClass& B = ctx->classes[cb];
+    for (int ck = 0; ck <= cb; ++ck) {
+      const PairClass& Kc = ctx->classes[ck];
+      const long kk = (long)B.Ka * B.Kb * Kc.Ka * Kc.Kb;
+      const int G = choose_group(B.la, B.lb, Kc.la, Kc.lb, kk);
+      const int qpw = 32 / G;
+      const double w = wmd_flops(B.la, B.lb, Kc.la, Kc.lb);
+      for (int i = B.first; i < B.first + B.count; ++i) {
+        const double qi = Q[i];
+        // number of kets with qi * qj > thr (Q sorted descending)
+        int lo = 0, hi = Kc.count;
+        while (lo < hi) {
+          const int mid = (lo + hi) / 2;
+          if (qi * Q[Kc.first + mid] > thr) lo = mid + 1; else hi = mid;
+        }
+        int nsig = lo;
+        if (cb == ck) nsig = std::min(nsig, i - B.first + 1);
+        if (nsig <= 0) continue;
+        int n64 = nsig;
+        if (precision == HFG_MIXED) {
+          lo = 0;
+          hi = nsig;
+          while (lo < hi) {
+            const int mid = (lo + hi) / 2;
+            if (qi * Q[Kc.first + mid] >= mixed) lo = mid + 1; else hi = mid;
+          }
+          n64 = lo;
+        }
+        const int ranges[2][2] = {{0, n64}, {n64, nsig}};
+        for (int r = 0; r < 2; ++r) {
+          const int a0 = ranges[r][0], a1 = ranges[r][1];
+          if (a1 <= a0) continue;
+          Launch& L = get_launch(B.la, B.lb, Kc.la, Kc.lb, G, r == 1);
+          L.entries.push_back({i, Kc.first + a0, Kc.first + a1, 0});
+          L.prefix.push_back(L.prefix.back() + (a1 - a0 + qpw - 1) / qpw);
+          const double nq = a1 - a0;
+          const double npr = ctx->h_pairs[i].npp * (cum[Kc.first + a1] - cum[Kc.first + a0]);
+          if (r == 0) {
+            st.quartets_fp64 += nq;
+            st.prim_quartets_fp64 += npr;
+            st.wmd_flops_fp64 += npr * w;
+          } else {
+            st.quartets_fp32 += nq;
+            st.prim_quartets_fp32 += npr;
+            st.wmd_flops_fp32 += npr * w;
+          }
+        }
+      }
+    }
+  }
+  // most expensive launches first
+  std::sort(plan->launches.begin(), plan->launches.end(), [](const Launch& x, const Launch& y) {
+    return std::make_tuple(x.la + x.lb + x.lc + x.ld, x.fp32) > std::make_tuple(y.la + y.lb + y.lc + y.ld, y.fp32);
+  });
+  for (auto& L : plan->launches) {
+    HFG_CUDA(ctx, cudaMalloc(&L.d_entries, L.entries.size() * sizeof(JKEntry)));
+    HFG_CUDA(ctx, cudaMalloc(&L.d_prefix, L.prefix.size() * sizeof(long long)));
+    HFG_CUDA(ctx, cudaMemcpy(L.d_entries, L.entries.data(), L.entries.size() * sizeof(JKEntry),
+                             cudaMemcpyHostToDevice));
+    HFG_CUDA(ctx, cudaMemcpy(L.d_prefix, L.prefix.data(), L.prefix.size() * sizeof(long long),
+                             cudaMemcpyHostToDevice));
+    // the host copies are no longer needed beyond the counts
+    const size_t ne = L.entries.size();
+    const long long nw = L.prefix.back();
+    L.entries.clear();
+    L.entries.shrink_to_fit();
+    L.prefix.assign({(long long)ne, nw});
+  }
+  st.launches = (int)plan->launches.size();
+  plan->stats = st;
+  out = plan.get();
+  ctx->plans[key] = std::move(plan);
+  return HFG_OK;
+}
+
+__global__ void symmetrize_kernel(const double* __restrict__ acc, double* __restrict__ out, int n, int nmat) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nn = (long long)n * n;
+  if (t >= nn * nmat) return;
+  const long long m = t / nn, r = t % nn;
+  const int i = (int)(r / n), j = (int)(r % n);
+  out[t] = 0.5 * (acc[m * nn + (long long)i * n + j] + acc[m * nn + (long long)j * n + i]);
+}
+
+__global__ void fock_kernel(const double* __restrict__ H, const double* __restrict__ J, const double* __restrict__ K,
+                            double* __restrict__ F, double kscale, long long nn) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nn) F[t] = H[t] + J[t] - kscale * K[t];
+}
+
+int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs,
+                     double* dJ, double* dK) {
+  hfg_jk_opts o;
+  if (opts) o = *opts; else hfg_jk_opts_default(&o);
+  if (nspin < 1 || nspin > 2) return set_error(ctx, HFG_ERR_INVALID_INPUT, "nspin must be 1 or 2");
+  if (!(o.schwarz_threshold >= 0.0) || !(o.prim_threshold >= 0.0) ||
+      (o.precision != HFG_FP64 && o.precision != HFG_MIXED))
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid J/K options");
+  Plan* plan = nullptr;
+  int rc = build_plan(ctx, o.schwarz_threshold, o.mixed_threshold, o.prim_threshold, o.precision, plan);
+  if (rc != HFG_OK) return rc;
+  const size_t nn = (size_t)ctx->n * ctx->n;
+  HFG_CUDA(ctx, ctx->d_Jacc.alloc(nn));
+  HFG_CUDA(ctx, ctx->d_Kacc.alloc(2 * nn));
+  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Jacc.p, 0, nn * sizeof(double), ctx->stream));
+  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Kacc.p, 0, nspin * nn * sizeof(double), ctx->stream));
+  JKLaunchArgs a{};
+  a.pairs = ctx->d_pairs.p;
+  a.prims = ctx->d_prims.p;
+  a.boys64 = ctx->d_boys64.p;
+  a.boys32 = ctx->d_boys32.p;
+  a.Dtot = dPt;
+  a.Dspin = dPs;
+  a.Jacc = ctx->d_Jacc.p;
+  a.Kacc = ctx->d_Kacc.p;
+  a.n = ctx->n;
+  a.nspin = nspin;
+  a.prim_eps = o.prim_threshold;
+  for (const auto& L : plan->launches) {
+    a.entries = L.d_entries;
+    a.prefix = L.d_prefix;
+    a.nentries = (int)L.prefix[0];
+    a.nwarps = L.prefix[1];
+    HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.G, L.fp32, a, ctx->stream));
+  }
+  const int blk = 256;
+  HFG_CUDA(ctx, (symmetrize_kernel<<<(unsigned)((nn + blk - 1) / blk), blk, 0, ctx->stream>>>(ctx->d_Jacc.p, dJ,
+                                                                                              ctx->n, 1),
+                 cudaGetLastError()));
+  HFG_CUDA(ctx, (symmetrize_kernel<<<(unsigned)((nspin * nn + blk - 1) / blk), blk, 0, ctx->stream>>>(
+                     ctx->d_Kacc.p, dK, ctx->n, nspin),
+                 cudaGetLastError()));
+  ctx->last = plan->stats;
+  return HFG_OK;
+}
+
+}  // namespace hfg
+
+hfg_ctx::~hfg_ctx() {
+  for (auto& kv : plans)
+    for (auto& L : kv.second->launches) {
+      if (L.d_entries) cudaFree(L.d_entries);
+      if (L.d_prefix) cudaFree(L.d_prefix);
+    }
+  d_pairs.release();
+  d_prims.release();
+  d_boys64.release();
+  d_boys32.release();
+  d_D.release();
+  d_Ds.release();
+  d_Jacc.release();
+  d_Kacc.release();
+  d_J.release();
+  d_K.release();
+  d_tmp.release();
+  if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+extern "C" {
+
+void hfg_jk_opts_default(hfg_jk_opts* o) {
+  if (!o) return;
+  o->schwarz_threshold = 1e-12;
+  o->prim_threshold = 0.0;
+  o->precision = HFG_FP64;
+  o->mixed_threshold = 1e-7;
+}
+
+int hfg_ctx_create(const hfg_basis* basis, int device, void* stream, hfg_ctx** out) {
+  if (!out) return HFG_ERR_INVALID_INPUT;
+  *out = nullptr;
+  auto ctx = std::make_unique<hfg_ctx>();
+  ctx->device = device;
+  int rc = cuda_check(ctx.get(), cudaSetDevice(device), "cudaSetDevice");
+  if (rc == HFG_OK) {
+    if (stream) ctx->stream = (cudaStream_t)stream;
+    else {
+      rc = cuda_check(ctx.get(), cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+      ctx->own_stream = true;
+    }
+  }
+  if (rc == HFG_OK) rc = build_shells(ctx.get(), basis);
+  if (rc == HFG_OK) {
+    const auto& t = boys_table_host();
+    std::vector<float> tf(t.begin(), t.end());
+    rc = cuda_check(ctx.get(), ctx->d_boys64.alloc(t.size()), "alloc boys");
+    if (rc == HFG_OK) rc = cuda_check(ctx.get(), ctx->d_boys32.alloc(tf.size()), "alloc boys32");
+    if (rc == HFG_OK)
+      rc = cuda_check(ctx.get(), cudaMemcpy(ctx->d_boys64.p, t.data(), t.size() * 8, cudaMemcpyHostToDevice), "boys");
+    if (rc == HFG_OK)
+      rc = cuda_check(ctx.get(), cudaMemcpy(ctx->d_boys32.p, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice),
+                      "boys32");
+  }
+  if (rc == HFG_OK) rc = build_pairs(ctx.get());
+  if (rc != HFG_OK) {
+    // keep the message for the caller through a minimal context
+    *out = ctx.release();
+    return rc;
+  }
+  *out = ctx.release();
+  return HFG_OK;
+}
+
+int hfg_ctx_destroy(hfg_ctx* ctx) {
+  if (!ctx) return HFG_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  delete ctx;
+  return HFG_OK;
+}
+
+const char* hfg_last_error(const hfg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int hfg_ctx_sizes(const hfg_ctx* ctx, int* n_ao, int* n_shell, long* n_pair) {
+  if (!ctx) return HFG_ERR_INVALID_INPUT;
+  if (n_ao) *n_ao = ctx->n;
+  if (n_shell) *n_shell = (int)ctx->shells.size();
+  if (n_pair) *n_pair = (long)ctx->ref_pairs.size();
+  return HFG_OK;
+}
+
+int hfg_schwarz(hfg_ctx* ctx, double* bounds, long n) {
+  if (!ctx || !bounds || n != (long)ctx->ref_pairs.size()) return set_error(ctx, HFG_ERR_INVALID_INPUT, "size");
+  for (long r = 0; r < n; ++r) bounds[r] = ctx->sorted_Q[ctx->ref_to_sorted[r]];
+  return HFG_OK;
+}
+
+int hfg_shell_quartet(hfg_ctx* ctx, int a, int b, int c, int d, double* out) {
+  if (!ctx || !out) return HFG_ERR_INVALID_INPUT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  const int ns = (int)ctx->shells.size();
+  for (int s : {a, b, c, d})
+    if (s < 0 || s >= ns) return set_error(ctx, HFG_ERR_INVALID_INPUT, "shell index out of range");
+  cudaSetDevice(ctx->device);
+  // orient each pair la >= lb; remember swaps to permute the block back
+  const bool sab = ctx->shells[a].l < ctx->shells[b].l, scd = ctx->shells[c].l < ctx->shells[d].l;
+  const int A = sab ? b : a, B = sab ? a : b, C = scd ? d : c, D = scd ? c : d;
+  PairInfo pi[2];
+  std::vector<PrimPair> pp;
+  make_pair(ctx, A, B, pi[0], pp, 0);
+  make_pair(ctx, C, D, pi[1], pp, 1);
+  const int na = ncart(ctx->shells[A].l), nb = ncart(ctx->shells[B].l), nc = ncart(ctx->shells[C].l),
+            nd = ncart(ctx->shells[D].l);
+  const size_t tot = (size_t)na * nb * nc * nd;
+  DevBuf<PairInfo> dpi;
+  DevBuf<PrimPair> dpp;
+  DevBuf<double> dout;
+  HFG_CUDA(ctx, dpi.alloc(2));
+  HFG_CUDA(ctx, dpp.alloc(pp.size()));
+  HFG_CUDA(ctx, dout.alloc(tot));
+  HFG_CUDA(ctx, cudaMemcpyAsync(dpi.p, pi, sizeof(pi), cudaMemcpyHostToDevice, ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(dpp.p, pp.data(), pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice, ctx->stream));
+  HFG_CUDA(ctx, launch_quartet(ctx->shells[A].l, ctx->shells[B].l, ctx->shells[C].l, ctx->shells[D].l, dpi.p, dpp.p,
+                               ctx->d_boys64.p, dout.p, ctx->stream));
+  std::vector<double> blk(tot);
+  HFG_CUDA(ctx, cudaMemcpyAsync(blk.data(), dout.p, tot * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  dpi.release();
+  dpp.release();
+  dout.release();
+  // permute (A B | C D) back to (a b | c d)
+  const int oa = ncart(ctx->shells[a].l), ob = ncart(ctx->shells[b].l), oc = ncart(ctx->shells[c].l),
+            od = ncart(ctx->shells[d].l);
+  for (int i = 0; i < oa; ++i)
+    for (int j = 0; j < ob; ++j)
+      for (int k = 0; k < oc; ++k)
+        for (int l = 0; l < od; ++l) {
+          const int I = sab ? j : i, J = sab ? i : j, K = scd ? l : k, L = scd ? k : l;
+          out[((i * ob + j) * oc + k) * od + l] = blk[((I * nb + J) * nc + K) * nd + L];
+        }
+  return HFG_OK;
+}
+
+int hfg_jk_device(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs, double* dJ,
+                  double* dK) {
+  if (!ctx || !dPt || !dPs || !dJ || !dK) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  return jk_device_locked(ctx, opts, nspin, dPt, dPs, dJ, dK);
+}
+
+int hfg_jk(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* Pt, const double* Ps, double* J,
+           double* K) {
+  if (!ctx || !Pt || !Ps || !J || !K) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  if (nspin < 1 || nspin > 2) return set_error(ctx, HFG_ERR_INVALID_INPUT, "nspin must be 1 or 2");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  const size_t nn = (size_t)ctx->n * ctx->n;
+  HFG_CUDA(ctx, ctx->d_D.alloc(nn));
+  HFG_CUDA(ctx, ctx->d_Ds.alloc(2 * nn));
+  HFG_CUDA(ctx, ctx->d_J.alloc(nn));
+  HFG_CUDA(ctx, ctx->d_K.alloc(2 * nn));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_D.p, Pt, nn * 8, cudaMemcpyHostToDevice, ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_Ds.p, Ps, nspin * nn * 8, cudaMemcpyHostToDevice, ctx->stream));
+  int rc = jk_device_locked(ctx, opts, nspin, ctx->d_D.p, ctx->d_Ds.p, ctx->d_J.p, ctx->d_K.p);
+  if (rc != HFG_OK) return rc;
+  HFG_CUDA(ctx, cudaMemcpyAsync(J, ctx->d_J.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(K, ctx->d_K.p, nspin * nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return HFG_OK;
+}
+
+static int fock_common(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* Pa, const double* Pb,
+                       double* Fa, double* Fb, int uhf) {
+  if (!ctx || !H || !Pa || !Fa || (uhf && (!Pb || !Fb))) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  const size_t nn = (size_t)ctx->n * ctx->n;
+  HFG_CUDA(ctx, ctx->d_D.alloc(nn));
+  HFG_CUDA(ctx, ctx->d_Ds.alloc(2 * nn));
+  HFG_CUDA(ctx, ctx->d_J.alloc(nn));
+  HFG_CUDA(ctx, ctx->d_K.alloc(2 * nn));
+  HFG_CUDA(ctx, ctx->d_tmp.alloc(3 * nn));
+  double* dH = ctx->d_tmp.p;
+  double* dF = ctx->d_tmp.p + nn;
+  HFG_CUDA(ctx, cudaMemcpyAsync(dH, H, nn * 8, cudaMemcpyHostToDevice, ctx->stream));
+  const int nspin = uhf ? 2 : 1;
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_Ds.p, Pa, nn * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (uhf) {
+    HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_Ds.p + nn, Pb, nn * 8, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  const double* dPt = ctx->d_Ds.p;
+  if (uhf) {
+    // P_total = Pa + Pb (the Fock kernel with a zero K weight)
+    fock_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, ctx->stream>>>(ctx->d_Ds.p, ctx->d_Ds.p + nn, ctx->d_Ds.p,
+                                                                        ctx->d_D.p, 0.0, (long long)nn);
+    HFG_CUDA(ctx, cudaGetLastError());
+    dPt = ctx->d_D.p;
+  }
+  int rc = jk_device_locked(ctx, opts, nspin, dPt, ctx->d_Ds.p, ctx->d_J.p, ctx->d_K.p);
+  if (rc != HFG_OK) return rc;
+  const double ks = uhf ? 1.0 : 0.5;
+  for (int s = 0; s < nspin; ++s) {
+    fock_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, ctx->stream>>>(dH, ctx->d_J.p, ctx->d_K.p + s * nn, dF, ks,
+                                                                        (long long)nn);
+    HFG_CUDA(ctx, cudaGetLastError());
+    HFG_CUDA(ctx, cudaMemcpyAsync(s == 0 ? Fa : Fb, dF, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return HFG_OK;
+}
+
+int hfg_fock_rhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* P, double* F) {
+  return fock_common(ctx, opts, H, P, nullptr, F, nullptr, 0);
+}
+
+int hfg_fock_uhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* Pa, const double* Pb,
+                 double* Fa, double* Fb) {
+  return fock_common(ctx, opts, H, Pa, Pb, Fa, Fb, 1);
+}
+
+int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* st) {
+  if (!ctx || !st) return HFG_ERR_INVALID_INPUT;
+  *st = ctx->last;
+  return HFG_OK;
+}
+
+}  // extern "C"

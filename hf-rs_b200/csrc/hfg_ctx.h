@@ -1,0 +1,100 @@
+// Host-side context of libhfg: the basis as shells, the shell-pair and
+// primitive-pair tables (device resident), and cached J/K launch plans.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/hfg.h"
+#include "hfg_internal.h"
+
+namespace hfg {
+
+struct Shell {
+  double c[3];
+  int l, K, ao, atom;
+  int prim_off;  // into hfg_ctx::exps / coefs (shell contraction coefficients)
+};
+
+struct PairClass {
+  int la, lb, Ka, Kb;
+  int first, count;  // range of the sorted global pair table
+};
+
+struct Launch {
+  int la, lb, lc, ld, G;
+  bool fp32;
+  std::vector<JKEntry> entries;
+  std::vector<long long> prefix;
+  JKEntry* d_entries = nullptr;
+  long long* d_prefix = nullptr;
+};
+
+struct Plan {
+  std::vector<Launch> launches;
+  hfg_jk_stats stats{};
+};
+
+// Device buffer owned by the context.
+template <typename T> struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t count) {
+    if (count <= n) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+}  // namespace hfg
+
+struct hfg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::mutex mu;
+  std::string err;
+
+  int n = 0;  // Cartesian functions
+  std::vector<hfg::Shell> shells;
+  std::vector<double> exps, coefs;
+  std::vector<std::pair<int, int>> ref_pairs;  // hf-rs order: (a, b), a >= b
+  std::vector<int> ref_to_sorted;             // hf-rs pair index -> sorted pair index
+  std::vector<double> sorted_Q;               // Schwarz bound per sorted pair
+  std::vector<hfg::PairInfo> h_pairs;         // sorted pair table
+  std::vector<hfg::PrimPair> h_prims;
+  std::vector<hfg::PairClass> classes;
+
+  hfg::DevBuf<hfg::PairInfo> d_pairs;
+  hfg::DevBuf<hfg::PrimPair> d_prims;
+  hfg::DevBuf<double> d_boys64;
+  hfg::DevBuf<float> d_boys32;
+  hfg::DevBuf<double> d_D, d_Ds, d_Jacc, d_Kacc, d_J, d_K, d_tmp;
+
+  std::map<std::tuple<double, double, double, int>, std::unique_ptr<hfg::Plan>> plans;
+  hfg_jk_stats last{};
+
+  ~hfg_ctx();
+};
+
+namespace hfg {
+// Implemented in ctx.cu, used by scf.cu.
+int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs,
+                     double* dJ, double* dK);
+int set_error(hfg_ctx* ctx, int code, const std::string& msg);
+int cuda_check(hfg_ctx* ctx, cudaError_t e, const char* what);
+}  // namespace hfg

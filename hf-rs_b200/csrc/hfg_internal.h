@@ -1,0 +1,56 @@
+// Internal data layout shared by the host runtime and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace hfg {
+
+constexpr int kLMax = 2;  // angular momentum built into the J/K kernels (s, p, d)
+
+// One shell pair, oriented so that la >= lb (and Ka >= Kb when la == lb).
+// 64 bytes.
+struct PairInfo {
+  double Ax, Ay, Az;     // centre of shell a
+  double ABx, ABy, ABz;  // A - B
+  int ao_a, ao_b;        // first Cartesian function of shell a / b
+  int pp_off, npp;       // primitive pairs [pp_off, pp_off + npp), sorted by bound
+  int same;              // shells a and b are the same shell
+  int cls;               // pair class index
+};
+
+// One primitive pair.  64 bytes.  kp = c_a c_b exp(-mu |AB|^2) / p with the
+// shell contraction coefficients (component scale factored out); the
+// Gaussian product centre is stored relative to centre A (P = A + PA), which
+// keeps P - Q accurate in FP32 as (A - C) + PA - QC.
+struct PrimPair {
+  double p, inv_p;
+  double PAx, PAy, PAz;
+  double kp;
+  double bound;  // sqrt(max_i (ab|ab)_ii) of this primitive pair alone
+  double pad;
+};
+
+// Work entry of one J/K launch: bra pair and the range of ket pairs
+// [k_lo, k_hi) (global pair indices, kets of one pair class).
+struct JKEntry {
+  int bra, k_lo, k_hi, pad;
+};
+
+struct JKLaunchArgs {
+  const JKEntry* entries;
+  const long long* prefix;  // warp-chunk prefix over entries (size nentries + 1)
+  int nentries;
+  long long nwarps;
+  const PairInfo* pairs;
+  const PrimPair* prims;
+  const double* boys64;
+  const float* boys32;
+  const double* Dtot;  // n x n
+  const double* Dspin; // nspin n x n
+  double* Jacc;        // n x n
+  double* Kacc;        // nspin n x n
+  int n, nspin;
+  double prim_eps;
+};
+
+}  // namespace hfg

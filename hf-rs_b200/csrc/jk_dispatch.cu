@@ -1,0 +1,74 @@
+// Dispatch tables for the J/K, Schwarz and single-quartet kernels.
+#include "jk_dispatch.h"
+#include "jk_kernels.cuh"
+
+namespace hfg {
+
+cudaError_t launch_jk(int la, int lb, int lc, int ld, int G, bool fp32, const JKLaunchArgs& a, cudaStream_t st) {
+#define HFG_CASE(A, B, C, D) \
+  if (la == A && lb == B && lc == C && ld == D) return launch_jk_##A##B##C##D(a, G, fp32, st);
+  HFG_CASE(0, 0, 0, 0)
+  HFG_CASE(1, 0, 0, 0)
+  HFG_CASE(1, 0, 1, 0)
+  HFG_CASE(1, 1, 0, 0)
+  HFG_CASE(1, 1, 1, 0)
+  HFG_CASE(1, 1, 1, 1)
+  HFG_CASE(2, 0, 0, 0)
+  HFG_CASE(2, 0, 1, 0)
+  HFG_CASE(2, 0, 1, 1)
+  HFG_CASE(2, 0, 2, 0)
+  HFG_CASE(2, 1, 0, 0)
+  HFG_CASE(2, 1, 1, 0)
+  HFG_CASE(2, 1, 1, 1)
+  HFG_CASE(2, 1, 2, 0)
+  HFG_CASE(2, 1, 2, 1)
+  HFG_CASE(2, 2, 0, 0)
+  HFG_CASE(2, 2, 1, 0)
+  HFG_CASE(2, 2, 1, 1)
+  HFG_CASE(2, 2, 2, 0)
+  HFG_CASE(2, 2, 2, 1)
+  HFG_CASE(2, 2, 2, 2)
+#undef HFG_CASE
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_schwarz(int la, int lb, const PairInfo* pairs, const PrimPair* prims, int first, int count,
+                           const double* boys, double* out, int prim_mode, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  const int block = 64, grid = (count + block - 1) / block;
+#define HFG_CASE(A, B)                                                                             \
+  if (la == A && lb == B) {                                                                        \
+    schwarz_kernel<A, B><<<grid, block, 0, st>>>(pairs, prims, first, count, boys, out, prim_mode); \
+    return cudaGetLastError();                                                                     \
+  }
+  HFG_CASE(0, 0)
+  HFG_CASE(1, 0)
+  HFG_CASE(1, 1)
+  HFG_CASE(2, 0)
+  HFG_CASE(2, 1)
+  HFG_CASE(2, 2)
+#undef HFG_CASE
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_quartet(int la, int lb, int lc, int ld, const PairInfo* pairs, const PrimPair* prims,
+                           const double* boys, double* out, cudaStream_t st) {
+#define HFG_CASE(A, B, C, D)                                                    \
+  if (la == A && lb == B && lc == C && ld == D) {                               \
+    quartet_kernel<A, B, C, D><<<1, 32, 0, st>>>(pairs, prims, boys, out);      \
+    return cudaGetLastError();                                                  \
+  }
+#define HFG_KET(A, B) \
+  HFG_CASE(A, B, 0, 0) HFG_CASE(A, B, 1, 0) HFG_CASE(A, B, 1, 1) HFG_CASE(A, B, 2, 0) HFG_CASE(A, B, 2, 1) HFG_CASE(A, B, 2, 2)
+  HFG_KET(0, 0)
+  HFG_KET(1, 0)
+  HFG_KET(1, 1)
+  HFG_KET(2, 0)
+  HFG_KET(2, 1)
+  HFG_KET(2, 2)
+#undef HFG_KET
+#undef HFG_CASE
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace hfg

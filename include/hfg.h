@@ -1,0 +1,132 @@
+/*
+ * hfg.h -- C ABI of the B200 Fock-build library (libhfg.so).
+ *
+ * Drop-in replacement, at the C level, for hf-rs's integral and Fock-build
+ * calls.  Each entry point names the hf-rs function it stands in for
+ * (paths relative to the hf-rs project root).  All host matrices are
+ * row-major doubles owned by the caller; device state lives behind the
+ * opaque handles.  Every call returns an hfg_status; hfg_last_error()
+ * gives the message of the last failure on a context.
+ *
+ * Threading: one context per CUDA stream.  Calls on one context are
+ * serialised by the context; different contexts may run concurrently.
+ */
+#ifndef HFG_H
+#define HFG_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; the first four mirror HfError (src/error.rs:6-15). */
+typedef enum {
+  HFG_OK = 0,
+  HFG_ERR_INVALID_INPUT = 1, /* HfError::InvalidInput */
+  HFG_ERR_INTEGRAL = 2,      /* HfError::Integral */
+  HFG_ERR_SCF = 3,           /* HfError::Scf (and the SCF drivers' Err(String)) */
+  HFG_ERR_OOM = 4,           /* device memory or admission budget exhausted */
+  HFG_ERR_TIMEOUT = 5,       /* a bounded device wait gave up */
+  HFG_ERR_CUDA = 6,          /* CUDA runtime / library failure */
+  HFG_ERR_UNSUPPORTED = 7    /* angular momentum or shape not built into this library */
+} hfg_status;
+
+/*
+ * A list of Cartesian contracted Gaussians, laid out exactly like hf-rs's
+ * Vec<ContractedGaussian> (src/basis.rs:87-100): per function its centre
+ * (bohr), Cartesian powers, atom index and primitives whose coefficients are
+ * fully normalised for that component (src/basis.rs:455-496).  Functions of
+ * one shell must be consecutive and complete, as build_basis emits them
+ * (src/ao.rs:133-164).
+ */
+typedef struct {
+  int n;                /* number of Cartesian functions */
+  const double* center; /* [n][3] */
+  const int* lxyz;      /* [n][3] */
+  const int* atom;      /* [n] */
+  const int* prim_off;  /* [n+1] offsets into exps/coefs */
+  const double* exps;   /* [prim_off[n]] */
+  const double* coefs;  /* [prim_off[n]] */
+} hfg_basis;
+
+typedef enum { HFG_FP64 = 0, HFG_MIXED = 1 } hfg_precision;
+
+typedef struct {
+  double schwarz_threshold; /* keep (ab|cd) iff Q_ab*Q_cd > this; hf-rs uses 1e-12
+                               (src/shell_integrals.rs:184) */
+  double prim_threshold;    /* drop primitive quartets whose Cauchy-Schwarz bound is
+                               below this; 0 reproduces hf-rs's quartet set exactly */
+  int precision;            /* hfg_precision */
+  double mixed_threshold;   /* HFG_MIXED: quartets with Q_ab*Q_cd below this are
+                               evaluated in FP32 and accumulated in FP64 */
+} hfg_jk_opts;
+
+typedef struct hfg_ctx hfg_ctx;
+
+/* Default options: Schwarz 1e-12, no primitive screening, FP64. */
+void hfg_jk_opts_default(hfg_jk_opts* opts);
+
+/*
+ * Creates a context for one basis on one device: groups the functions into
+ * shells, builds the shell-pair and primitive-pair tables and the Schwarz
+ * bounds Q_ab = sqrt(max_i (ab|ab)_ii) on the device (src/shell_integrals.rs:
+ * 156-173).  `stream` is a cudaStream_t (NULL = a stream owned by the
+ * context).
+ */
+int hfg_ctx_create(const hfg_basis* basis, int device, void* stream, hfg_ctx** out);
+int hfg_ctx_destroy(hfg_ctx* ctx);
+const char* hfg_last_error(const hfg_ctx* ctx);
+
+/* Basic sizes: Cartesian functions, shells, shell pairs. */
+int hfg_ctx_sizes(const hfg_ctx* ctx, int* n_ao, int* n_shell, long* n_pair);
+
+/* Schwarz bounds in hf-rs shell-pair order (a >= b, row by row). */
+int hfg_schwarz(hfg_ctx* ctx, double* bounds, long n);
+
+/*
+ * Stands in for compute_shell_quartet (src/shell_integrals.rs:138-151):
+ * the contracted Cartesian block (ab|cd) for shells a,b,c,d of the context
+ * basis, a,b,c,d row-major.  `out` holds n_a*n_b*n_c*n_d doubles.
+ */
+int hfg_shell_quartet(hfg_ctx* ctx, int a, int b, int c, int d, double* out);
+
+/*
+ * Stands in for compute_eri_tensor (src/scf.rs:275) followed by
+ * contract_jk (src/scf.rs:337-364), without storing the integrals: a direct
+ * J/K build from densities.  P_total (n x n) gives J; P_spin holds nspin
+ * n x n densities giving nspin K matrices (nspin = 1: RHF, K from P_total
+ * passed again; nspin = 2: UHF alpha/beta).  Host pointers; the call copies
+ * inputs to the device, builds, and copies J and K back.
+ */
+int hfg_jk(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* P_total, const double* P_spin,
+           double* J, double* K);
+
+/* As hfg_jk with device pointers, on the context stream, without copies. */
+int hfg_jk_device(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* d_P_total,
+                  const double* d_P_spin, double* d_J, double* d_K);
+
+/* Stands in for build_fock_matrix (src/scf.rs:366-369): F = H + J - K/2. */
+int hfg_fock_rhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* P, double* F);
+
+/* Stands in for build_uhf_fock_matrices (src/scf.rs:371-375):
+   F_a = H + J - K_a, F_b = H + J - K_b with J from P_a + P_b. */
+int hfg_fock_uhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* Pa, const double* Pb,
+                 double* Fa, double* Fb);
+
+/* Work counters of the last J/K build on this context: shell quartets and
+   primitive quartets evaluated in FP64 and FP32, and W_MD-weighted flops
+   (the McMurchie-Davidson count per primitive quartet of each class). */
+typedef struct {
+  double quartets_fp64, quartets_fp32;
+  double prim_quartets_fp64, prim_quartets_fp32;
+  double wmd_flops_fp64, wmd_flops_fp32;
+  int launches;
+} hfg_jk_stats;
+int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HFG_H */
