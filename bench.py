@@ -1,0 +1,406 @@
+"""Benchmark: direct Fock builds per second, (H2O)_64 cc-pVDZ, on B200.
+
+A step is one Fock build: the direct J and K of a closed-shell density
+(hfg_jk_device: Schwarz-screened four-centre ERIs digested into J/K, plus
+the symmetrisation epilogue) for the synthetic water cluster (H2O)_64 in
+cc-pVDZ (1600 Cartesian functions).  `value` is the mixed-precision build
+(FP32 for shell quartets with Q_ab Q_cd below the FP32 threshold, FP64
+accumulation) with the density resident in HBM; the same builds in plain
+FP64 are reported beside it.  `e2e` is the same build through the C ABI
+with host buffers (hfg_jk): density host->device, J and K device->host.
+
+Under torchrun each rank builds its own replica (weak scaling, no data-path
+collective); the step time is the maximum over ranks.
+
+--impl reference times the CPU restatement of hf-rs's path (the oracle:
+the same screened shell quartets, McMurchie-Davidson integrals, contract_jk
+digestion) on this host's cores on a bounded sample of the same build and
+scales it to whole builds by the share of McMurchie-Davidson work sampled.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hf-rs_b200"))
+
+METRIC = "fock_builds_per_s"
+UNIT = "Fock builds/s"
+WORKLOAD = "(H2O)64 cc-pVDZ direct RHF Fock build (J+K), 1600 Cartesian AOs, Schwarz 1e-12"
+SCHWARZ = 1e-12
+PRIM = 1e-15
+MIXED = 1e-7
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--waters", type=int, default=64)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def timed(torch, stream, fn, steps, flush=None):
+    """Per-step device time (ms) with CUDA events on `stream`."""
+    times = []
+    for _ in range(steps):
+        if flush is not None:
+            flush()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    return times
+
+
+class CpuWorkload:
+    """The oracle (CPU restatement of hf-rs) on the same build: the screened
+    shell quartets, their McMurchie-Davidson work, and timed samples of bra
+    shell-pair rows."""
+
+    W = {(0, 0, 0, 0): 61, (1, 0, 0, 0): 126, (1, 0, 1, 0): 333, (1, 1, 0, 0): 327, (1, 1, 1, 0): 1072,
+         (1, 1, 1, 1): 3916, (2, 0, 0, 0): 256, (2, 0, 1, 0): 771, (2, 0, 1, 1): 2683, (2, 0, 2, 0): 1872,
+         (2, 1, 0, 0): 747, (2, 1, 1, 0): 2647, (2, 1, 1, 1): 9994, (2, 1, 2, 0): 6751, (2, 1, 2, 1): 25570,
+         (2, 2, 0, 0): 1776, (2, 2, 1, 0): 6607, (2, 2, 1, 1): 25354, (2, 2, 2, 0): 16978, (2, 2, 2, 1): 64681,
+         (2, 2, 2, 2): 162643}
+
+    def __init__(self, atoms, threads):
+        import numpy as np
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        self.np, self.O = np, O
+        os.environ["ORACLE_THREADS"] = str(threads)
+        self.threads = threads
+        self.basis = O.build_basis(atoms, O.load_basis("cc-pvdz"))
+        self.fb = O.FlatBasis(self.basis)
+        shells = O.shell_ranges(self.basis)
+        L = np.array([sum(self.basis[s]["l"]) for s, _ in shells])
+        K = np.array([len(self.basis[s]["exps"]) for s, _ in shells])
+        self.Q = O.schwarz(self.basis)
+        a_idx, b_idx = [], []
+        for a in range(len(shells)):
+            for b in range(a + 1):
+                a_idx.append(a)
+                b_idx.append(b)
+        pa, pb = np.array(a_idx), np.array(b_idx)
+        self.code = np.maximum(L[pa], L[pb]) * 3 + np.minimum(L[pa], L[pb])
+        self.npp = (K[pa] * K[pb]).astype(np.float64)
+        self.wtab = np.zeros((9, 9))
+        for (a, b, c, d), v in self.W.items():
+            self.wtab[a * 3 + b, c * 3 + d] = v
+            self.wtab[c * 3 + d, a * 3 + b] = v
+        self.total = self._total_work()
+        n = len(self.basis)
+        rng = np.random.default_rng(7)
+        P = rng.standard_normal((n, n)) * 0.1
+        self.P = P + P.T
+        self.rng = rng
+        self.rate = None
+
+    def _total_work(self):
+        # sum over unique quartets ij >= kl with Q_ij Q_kl > thr of
+        # npp_ij npp_kl W(class): half the ordered double sum plus half the
+        # diagonal, the double sum by sorted prefixes per angular class.
+        np = self.np
+        tot = 0.0
+        for c in range(9):
+            sel = np.nonzero(self.code == c)[0]
+            if len(sel) == 0:
+                continue
+            o = sel[np.argsort(-self.Q[sel], kind="stable")]
+            qs, cum = self.Q[o], np.concatenate([[0.0], np.cumsum(self.npp[o])])
+            # count of kets with Q_ij * q > thr
+            cnt = np.searchsorted(-qs, -(SCHWARZ / np.maximum(self.Q, 1e-300)), side="left")
+            # exact predicate fix-up at the boundary
+            for _ in range(2):
+                over = (cnt < len(qs))
+                nxt = np.where(over, qs[np.minimum(cnt, len(qs) - 1)] * self.Q > SCHWARZ, False)
+                cnt = cnt + nxt
+                under = cnt > 0
+                prv = np.where(under, qs[np.maximum(cnt - 1, 0)] * self.Q <= SCHWARZ, False)
+                cnt = cnt - prv
+            tot += float(np.sum(self.npp * cum[cnt] * self.wtab[self.code, c]))
+        diag = self.Q * self.Q > SCHWARZ
+        tot += float(np.sum((self.npp ** 2 * self.wtab[self.code, self.code])[diag]))
+        return 0.5 * tot
+
+    def row_work(self, ij):
+        np = self.np
+        ks = np.nonzero(self.Q[ij] * self.Q[:ij + 1] > SCHWARZ)[0]
+        return float(np.sum(self.npp[ij] * self.npp[ks] * self.wtab[self.code[ij], self.code[ks]]))
+
+    def sample(self, target_s):
+        """Time the oracle on random rows worth ~target_s seconds; returns
+        (seconds, sampled work, rows)."""
+        np = self.np
+        if self.rate is None:
+            probe = self.rng.permutation(len(self.Q))[:8]
+            t0 = time.time()
+            self.O.direct_jk(self.basis, self.P, [self.P], SCHWARZ, rows=probe, fb=self.fb)
+            self.rate = max(sum(self.row_work(r) for r in probe) / max(time.time() - t0, 1e-3), 1.0)
+        rows, w = [], 0.0
+        for r in self.rng.permutation(len(self.Q)):
+            rows.append(int(r))
+            w += self.row_work(r)
+            if w / self.rate >= target_s or len(rows) >= 200000:
+                break
+        t0 = time.time()
+        self.O.direct_jk(self.basis, self.P, [self.P], SCHWARZ, rows=np.array(rows), fb=self.fb)
+        dt = time.time() - t0
+        self.rate = w / dt
+        return dt, w, len(rows)
+
+    def builds_per_s(self, target_s):
+        dt, w, nrows = self.sample(target_s)
+        return (w / self.total) / dt, dt, nrows
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from hfgpu.clusters import water_cluster
+    threads = os.cpu_count() or 1
+    cw = CpuWorkload(water_cluster(args.waters), threads)
+    per_step = min(15.0, 150.0 / max(1, args.steps + args.warmup))
+    vals, rows = [], 0
+    for s in range(args.warmup + args.steps):
+        v, dt, nrows = cw.builds_per_s(per_step)
+        if s >= args.warmup:
+            vals.append(v)
+            rows = nrows
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD + ", CPU restatement of hf-rs (McMurchie-Davidson, contract_jk)",
+                       "parallelism": "openmp-%d" % threads},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "%d random bra shell-pair rows per step (~%.0f s of CPU work), scaled by "
+                                       "sampled / total McMurchie-Davidson flops (%.3e per build)"
+                                       % (rows, per_step, cw.total)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from hfgpu import CartesianBasis, Context, JKOptions
+    from hfgpu.clusters import water_cluster
+    from hfgpu.lib import fma_peak_tflops
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    # one non-default stream shared by torch and the library, so the CUDA
+    # events below bracket the library's kernels
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    atoms = water_cluster(args.waters)
+    basis = CartesianBasis.build(atoms, "cc-pvdz")
+    n = basis.n
+    ctx = Context(basis, device=local, stream=stream.cuda_stream)
+    rng = np.random.default_rng(11)
+    Ph = rng.standard_normal((n, n)) * 0.1
+    Ph = Ph + Ph.T
+    P = torch.from_numpy(Ph).to(dev)
+    J = torch.empty((n, n), dtype=torch.float64, device=dev)
+    K = torch.empty((n, n), dtype=torch.float64, device=dev)
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def flush():
+        flush_buf.zero_()
+
+    opt_mixed = JKOptions.make(schwarz=SCHWARZ, prim=PRIM, mixed=MIXED)
+    opt_fp64 = JKOptions.make(schwarz=SCHWARZ, prim=PRIM)
+
+    def build(opt):
+        return lambda: ctx.jk_device(P.data_ptr(), P.data_ptr(), J.data_ptr(), K.data_ptr(), 1, opt)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (plans are built on first use)
+    for _ in range(args.warmup):
+        build(opt_mixed)()
+        build(opt_fp64)()
+    torch.cuda.synchronize()
+    stats_mixed = None
+    build(opt_mixed)()
+    stats_mixed = ctx.last_stats()
+    Jm, Km = J.cpu().numpy().copy(), K.cpu().numpy().copy()
+    build(opt_fp64)()
+    stats_fp64 = ctx.last_stats()
+    Jf, Kf = J.cpu().numpy().copy(), K.cpu().numpy().copy()
+    jk_diff = float(max(np.max(np.abs(Jm - Jf)), np.max(np.abs(Km - Kf))))
+
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    t_mixed = timed(torch, stream, build(opt_mixed), args.steps, flush)
+    barrier()
+    t_fp64 = timed(torch, stream, build(opt_fp64), args.steps, flush)
+    barrier()
+    ck = clocks.stop()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    tot_mixed = max_over_ranks(sum(t_mixed))
+    tot_fp64 = max_over_ranks(sum(t_fp64))
+    value = world * args.steps / (tot_mixed / 1000.0)
+    value_fp64 = world * args.steps / (tot_fp64 / 1000.0)
+
+    e2e = None
+    if not args.no_e2e:
+        Phost = torch.from_numpy(Ph).pin_memory()
+        Jh = torch.empty((n, n), dtype=torch.float64).pin_memory()
+        Kh = torch.empty((n, n), dtype=torch.float64).pin_memory()
+        import ctypes
+        lib = ctx.lib
+        DP = ctypes.POINTER(ctypes.c_double)
+
+        def e2e_step():
+            rc = lib.hfg_jk(ctx.h, ctypes.byref(opt_mixed), 1, ctypes.cast(Phost.data_ptr(), DP),
+                            ctypes.cast(Phost.data_ptr(), DP), ctypes.cast(Jh.data_ptr(), DP),
+                            ctypes.cast(Kh.data_ptr(), DP))
+            if rc != 0:
+                raise RuntimeError(lib.hfg_last_error(ctx.h).decode())
+
+        e2e_step()
+        barrier()
+        t_e2e = timed(torch, stream, e2e_step, args.steps, flush)
+        barrier()
+        tot_e2e = max_over_ranks(sum(t_e2e))
+        e2e = {"value": world * args.steps / (tot_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": n * n * 8,
+               "d2h_bytes_per_step": 2 * n * n * 8, "ms_per_step": tot_e2e / args.steps}
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    p64 = fma_peak_tflops(local, False)
+    p32 = fma_peak_tflops(local, True)
+    t_step = tot_mixed / args.steps / 1000.0
+    pipe_frac = (stats_mixed["wmd_flops_fp64"] / (p64 * 1e12) + stats_mixed["wmd_flops_fp32"] / (p32 * 1e12)) / t_step
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "jk_kernels_h2o64.txt")
+    if os.path.exists(prof):
+        for ln in open(prof):
+            if ln.startswith("traffic_bytes_per_build:"):
+                traffic = float(ln.split(":")[1])
+    roofline = {"bound": "fp64", "achieved": pipe_frac * p64, "peak": p64, "unit": "TFLOP/s", "frac": pipe_frac,
+                "traffic": traffic,
+                "peak_source": "measured FMA chains on this device (hfg_fma_peak); FP32 work weighted by the "
+                               "measured FP32 peak %.1f TFLOP/s" % p32,
+                "work_unit": "McMurchie-Davidson flops per evaluated primitive quartet (hf-rs loops), "
+                             "%.3e FP64 + %.3e FP32 per build" % (stats_mixed["wmd_flops_fp64"],
+                                                                   stats_mixed["wmd_flops_fp32"])}
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        try:
+            cw = CpuWorkload(atoms, os.cpu_count() or 1)
+            v, dt, nrows = cw.builds_per_s(15.0)
+            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                   "sample": "%d random bra shell-pair rows of the same build (%.1f s), scaled by sampled / "
+                             "total McMurchie-Davidson flops (%.3e per build)" % (nrows, dt, cw.total)}
+        except Exception as exc:  # the CPU leg must not hide the GPU result
+            cpu = {"unavailable": str(exc)[:200]}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot_mixed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32-mixed", "data": "synthetic",
+            "config": {"workload": WORKLOAD + ", mixed precision (FP32 below Q_ab*Q_cd < %g), primitive "
+                                              "screening %g" % (MIXED, PRIM),
+                       "n_ao": n, "waters": args.waters, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "flushed (256 MB write) before every timed step"},
+            "fp64": {"value": value_fp64, "unit": UNIT, "ms_per_step": tot_fp64 / args.steps,
+                     "wmd_flops": stats_fp64["wmd_flops_fp64"]},
+            "mixed_over_fp64": value / value_fp64, "jk_max_abs_diff_mixed_vs_fp64": jk_diff,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
+            "gpu_launches": args.steps * 2 * (stats_mixed["launches"] + 2) + args.steps * (stats_fp64["launches"] + 2)}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -244,11 +246,11 @@ static int build_pairs(hfg_ctx* ctx) {
   HFG_CUDA(ctx, dpb.alloc(gprim.size()));
   for (const auto& c : cls) {
     HFG_CUDA(ctx, launch_schwarz(c.la, c.lb, ctx->d_pairs.p, ctx->d_prims.p, c.first, c.count, ctx->d_boys64.p,
-                                 dq.p + c.first, 0, ctx->stream));
+                                 ctx->d_expt64.p, dq.p + c.first, 0, ctx->stream));
     const int p0 = gp[c.first].pp_off;
     const int p1 = gp[c.first + c.count - 1].pp_off + gp[c.first + c.count - 1].npp;
     HFG_CUDA(ctx, launch_schwarz(c.la, c.lb, ctx->d_pairs.p, ctx->d_prims.p, p0, p1 - p0, ctx->d_boys64.p,
-                                 dpb.p + p0, 1, ctx->stream));
+                                 ctx->d_expt64.p, dpb.p + p0, 1, ctx->stream));
   }
   std::vector<double> Q(gp.size()), PB(gprim.size());
   HFG_CUDA(ctx, cudaMemcpyAsync(Q.data(), dq.p, Q.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -286,6 +288,31 @@ static int build_pairs(hfg_ctx* ctx) {
                                 cudaMemcpyHostToDevice, ctx->stream));
   HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_prims.p, ctx->h_prims.data(), ctx->h_prims.size() * sizeof(PrimPair),
                                 cudaMemcpyHostToDevice, ctx->stream));
+  // compact records for the J/K kernels
+  const size_t npp = ctx->h_prims.size();
+  std::vector<PrimRec64> r64(npp);
+  std::vector<PrimRec32> r32(npp);
+  std::vector<float> pb(npp);
+  for (const auto& pi : ctx->h_pairs) {
+    const double ab2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
+    for (int k = 0; k < pi.npp; ++k) {
+      const PrimPair& q = ctx->h_prims[pi.pp_off + k];
+      // P - A = -(beta/p) AB; recover beta/p from the stored P - A
+      double bp = 0.0;
+      if (ab2 > 0.0) bp = -(q.PAx * pi.ABx + q.PAy * pi.ABy + q.PAz * pi.ABz) / ab2;
+      r64[pi.pp_off + k] = {q.p, q.inv_p, q.kp, bp};
+      r32[pi.pp_off + k] = {(float)q.p, (float)q.inv_p, (float)q.kp, (float)bp};
+      pb[pi.pp_off + k] = (float)q.bound;
+    }
+  }
+  HFG_CUDA(ctx, ctx->d_rec64.alloc(npp));
+  HFG_CUDA(ctx, ctx->d_rec32.alloc(npp));
+  HFG_CUDA(ctx, ctx->d_pbound.alloc(npp));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_rec64.p, r64.data(), npp * sizeof(PrimRec64), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_rec32.p, r32.data(), npp * sizeof(PrimRec32), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_pbound.p, pb.data(), npp * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return HFG_OK;
 }
@@ -329,9 +356,7 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     const PairClass& B = ctx->classes[cb];
     for (int ck = 0; ck <= cb; ++ck) {
       const PairClass& Kc = ctx->classes[ck];
-      const long kk = (long)B.Ka * B.Kb * Kc.Ka * Kc.Kb;
-      const int G = choose_group(B.la, B.lb, Kc.la, Kc.lb, kk);
-      const int qpw = 32 / G;
+      const int qpw = 32;
       const double w = wmd_flops(B.la, B.lb, Kc.la, Kc.lb);
       for (int i = B.first; i < B.first + B.count; ++i) {
         const double qi = Q[i];
@@ -358,11 +383,13 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
         for (int r = 0; r < 2; ++r) {
           const int a0 = ranges[r][0], a1 = ranges[r][1];
           if (a1 <= a0) continue;
-          Launch& L = get_launch(B.la, B.lb, Kc.la, Kc.lb, G, r == 1);
+          Launch& L = get_launch(B.la, B.lb, Kc.la, Kc.lb, 1, r == 1);
           L.entries.push_back({i, Kc.first + a0, Kc.first + a1, 0});
           L.prefix.push_back(L.prefix.back() + (a1 - a0 + qpw - 1) / qpw);
           const double nq = a1 - a0;
           const double npr = ctx->h_pairs[i].npp * (cum[Kc.first + a1] - cum[Kc.first + a0]);
+          L.quartets += nq;
+          L.prims += npr;
           if (r == 0) {
             st.quartets_fp64 += nq;
             st.prim_quartets_fp64 += npr;
@@ -393,6 +420,34 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     L.entries.clear();
     L.entries.shrink_to_fit();
     L.prefix.assign({(long long)ne, nw});
+  }
+  if (prim_eps > 0.0) {
+    // exact primitive-quartet counts after primitive screening
+    DevBuf<unsigned long long> cnt;
+    HFG_CUDA(ctx, cnt.alloc(plan->launches.size()));
+    HFG_CUDA(ctx, cudaMemsetAsync(cnt.p, 0, plan->launches.size() * 8, ctx->stream));
+    for (size_t l = 0; l < plan->launches.size(); ++l) {
+      const Launch& L = plan->launches[l];
+      HFG_CUDA(ctx, launch_count(L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1], ctx->d_pairs.p,
+                                 ctx->d_pbound.p, prim_eps, cnt.p + l, ctx->stream));
+    }
+    std::vector<unsigned long long> h(plan->launches.size());
+    HFG_CUDA(ctx, cudaMemcpyAsync(h.data(), cnt.p, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cnt.release();
+    st.prim_quartets_fp64 = st.prim_quartets_fp32 = st.wmd_flops_fp64 = st.wmd_flops_fp32 = 0.0;
+    for (size_t l = 0; l < plan->launches.size(); ++l) {
+      Launch& L = plan->launches[l];
+      L.prims = (double)h[l];
+      const double w = wmd_flops(L.la, L.lb, L.lc, L.ld);
+      if (L.fp32) {
+        st.prim_quartets_fp32 += (double)h[l];
+        st.wmd_flops_fp32 += (double)h[l] * w;
+      } else {
+        st.prim_quartets_fp64 += (double)h[l];
+        st.wmd_flops_fp64 += (double)h[l] * w;
+      }
+    }
   }
   st.launches = (int)plan->launches.size();
   plan->stats = st;
@@ -432,11 +487,17 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   HFG_CUDA(ctx, ctx->d_Kacc.alloc(2 * nn));
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Jacc.p, 0, nn * sizeof(double), ctx->stream));
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Kacc.p, 0, nspin * nn * sizeof(double), ctx->stream));
+  HFG_CUDA(ctx, ctx->d_counters.alloc(plan->launches.size() + 1));
+  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.p, 0, (plan->launches.size() + 1) * 8, ctx->stream));
   JKLaunchArgs a{};
   a.pairs = ctx->d_pairs.p;
-  a.prims = ctx->d_prims.p;
+  a.rec64 = ctx->d_rec64.p;
+  a.rec32 = ctx->d_rec32.p;
+  a.pbound = ctx->d_pbound.p;
   a.boys64 = ctx->d_boys64.p;
   a.boys32 = ctx->d_boys32.p;
+  a.expt64 = ctx->d_expt64.p;
+  a.expt32 = ctx->d_expt32.p;
   a.Dtot = dPt;
   a.Dspin = dPs;
   a.Jacc = ctx->d_Jacc.p;
@@ -444,12 +505,38 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   a.n = ctx->n;
   a.nspin = nspin;
   a.prim_eps = o.prim_threshold;
-  for (const auto& L : plan->launches) {
+  // HFG_PROFILE=1: per-launch device time (CUDA events) on stderr
+  static const bool profile = getenv("HFG_PROFILE") && getenv("HFG_PROFILE")[0] == '1';
+  std::vector<cudaEvent_t> ev;
+  if (profile) {
+    ev.resize(plan->launches.size() + 1);
+    for (auto& x : ev) cudaEventCreate(&x);
+    cudaEventRecord(ev[0], ctx->stream);
+  }
+  for (size_t l = 0; l < plan->launches.size(); ++l) {
+    const Launch& L = plan->launches[l];
+    a.counter = ctx->d_counters.p + l;
     a.entries = L.d_entries;
     a.prefix = L.d_prefix;
     a.nentries = (int)L.prefix[0];
     a.nwarps = L.prefix[1];
-    HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.G, L.fp32, a, ctx->stream));
+    HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.fp32, a, ctx->stream));
+    if (profile) cudaEventRecord(ev[l + 1], ctx->stream);
+  }
+  if (profile) {
+    cudaEventSynchronize(ev.back());
+    double tot = 0;
+    for (size_t l = 0; l < plan->launches.size(); ++l) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[l], ev[l + 1]);
+      tot += ms;
+      const Launch& L = plan->launches[l];
+      fprintf(stderr, "hfg-profile (%d%d|%d%d) %s entries %8lld warps %10lld quartets %.3e prims %.3e  %9.3f ms  %.3e prim/s\n",
+              L.la, L.lb, L.lc, L.ld, L.fp32 ? "fp32" : "fp64", L.prefix[0], L.prefix[1], L.quartets, L.prims, ms,
+              L.prims / (ms * 1e-3));
+    }
+    fprintf(stderr, "hfg-profile total %.3f ms\n", tot);
+    for (auto& x : ev) cudaEventDestroy(x);
   }
   const int blk = 256;
   HFG_CUDA(ctx, (symmetrize_kernel<<<(unsigned)((nn + blk - 1) / blk), blk, 0, ctx->stream>>>(ctx->d_Jacc.p, dJ,
@@ -472,8 +559,14 @@ hfg_ctx::~hfg_ctx() {
     }
   d_pairs.release();
   d_prims.release();
+  d_rec64.release();
+  d_rec32.release();
+  d_pbound.release();
   d_boys64.release();
   d_boys32.release();
+  d_expt64.release();
+  d_expt32.release();
+  d_counters.release();
   d_D.release();
   d_Ds.release();
   d_Jacc.release();
@@ -518,6 +611,20 @@ int hfg_ctx_create(const hfg_basis* basis, int device, void* stream, hfg_ctx** o
     if (rc == HFG_OK)
       rc = cuda_check(ctx.get(), cudaMemcpy(ctx->d_boys32.p, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice),
                       "boys32");
+    std::vector<double> e64(kBoysRows);
+    std::vector<float> e32(kBoysRows);
+    for (int i = 0; i < kBoysRows; ++i) {
+      e64[i] = std::exp(-i * kBoysStep);
+      e32[i] = (float)e64[i];
+    }
+    if (rc == HFG_OK) rc = cuda_check(ctx.get(), ctx->d_expt64.alloc(kBoysRows), "alloc expt");
+    if (rc == HFG_OK) rc = cuda_check(ctx.get(), ctx->d_expt32.alloc(kBoysRows), "alloc expt32");
+    if (rc == HFG_OK)
+      rc = cuda_check(ctx.get(), cudaMemcpy(ctx->d_expt64.p, e64.data(), kBoysRows * 8, cudaMemcpyHostToDevice),
+                      "expt");
+    if (rc == HFG_OK)
+      rc = cuda_check(ctx.get(), cudaMemcpy(ctx->d_expt32.p, e32.data(), kBoysRows * 4, cudaMemcpyHostToDevice),
+                      "expt32");
   }
   if (rc == HFG_OK) rc = build_pairs(ctx.get());
   if (rc != HFG_OK) {
@@ -579,7 +686,7 @@ int hfg_shell_quartet(hfg_ctx* ctx, int a, int b, int c, int d, double* out) {
   HFG_CUDA(ctx, cudaMemcpyAsync(dpi.p, pi, sizeof(pi), cudaMemcpyHostToDevice, ctx->stream));
   HFG_CUDA(ctx, cudaMemcpyAsync(dpp.p, pp.data(), pp.size() * sizeof(PrimPair), cudaMemcpyHostToDevice, ctx->stream));
   HFG_CUDA(ctx, launch_quartet(ctx->shells[A].l, ctx->shells[B].l, ctx->shells[C].l, ctx->shells[D].l, dpi.p, dpp.p,
-                               ctx->d_boys64.p, dout.p, ctx->stream));
+                               ctx->d_boys64.p, ctx->d_expt64.p, dout.p, ctx->stream));
   std::vector<double> blk(tot);
   HFG_CUDA(ctx, cudaMemcpyAsync(blk.data(), dout.p, tot * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -619,8 +726,10 @@ int hfg_jk(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* Pt, c
   HFG_CUDA(ctx, ctx->d_J.alloc(nn));
   HFG_CUDA(ctx, ctx->d_K.alloc(2 * nn));
   HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_D.p, Pt, nn * 8, cudaMemcpyHostToDevice, ctx->stream));
-  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_Ds.p, Ps, nspin * nn * 8, cudaMemcpyHostToDevice, ctx->stream));
-  int rc = jk_device_locked(ctx, opts, nspin, ctx->d_D.p, ctx->d_Ds.p, ctx->d_J.p, ctx->d_K.p);
+  // RHF callers pass the same matrix twice: copy it once
+  const bool same = (nspin == 1 && Ps == Pt);
+  if (!same) HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_Ds.p, Ps, nspin * nn * 8, cudaMemcpyHostToDevice, ctx->stream));
+  int rc = jk_device_locked(ctx, opts, nspin, ctx->d_D.p, same ? ctx->d_D.p : ctx->d_Ds.p, ctx->d_J.p, ctx->d_K.p);
   if (rc != HFG_OK) return rc;
   HFG_CUDA(ctx, cudaMemcpyAsync(J, ctx->d_J.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
   HFG_CUDA(ctx, cudaMemcpyAsync(K, ctx->d_K.p, nspin * nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -675,6 +784,12 @@ int hfg_fock_rhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const d
 int hfg_fock_uhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* Pa, const double* Pb,
                  double* Fa, double* Fb) {
   return fock_common(ctx, opts, H, Pa, Pb, Fa, Fb, 1);
+}
+
+int hfg_fma_peak(int device, int fp32, double* tflops) {
+  if (!tflops) return HFG_ERR_INVALID_INPUT;
+  if (cudaSetDevice(device) != cudaSuccess) return HFG_ERR_CUDA;
+  return fma_peak(fp32, tflops) == cudaSuccess ? HFG_OK : HFG_ERR_CUDA;
 }
 
 int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* st) {

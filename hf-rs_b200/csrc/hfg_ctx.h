@@ -29,6 +29,7 @@ struct PairClass {
 struct Launch {
   int la, lb, lc, ld, G;
   bool fp32;
+  double quartets = 0, prims = 0;  // shell quartets and primitive quartets (after screening) of this launch
   std::vector<JKEntry> entries;
   std::vector<long long> prefix;
   JKEntry* d_entries = nullptr;
@@ -81,8 +82,12 @@ struct hfg_ctx {
 
   hfg::DevBuf<hfg::PairInfo> d_pairs;
   hfg::DevBuf<hfg::PrimPair> d_prims;
-  hfg::DevBuf<double> d_boys64;
-  hfg::DevBuf<float> d_boys32;
+  hfg::DevBuf<hfg::PrimRec64> d_rec64;
+  hfg::DevBuf<hfg::PrimRec32> d_rec32;
+  hfg::DevBuf<float> d_pbound;
+  hfg::DevBuf<double> d_boys64, d_expt64;
+  hfg::DevBuf<float> d_boys32, d_expt32;
+  hfg::DevBuf<unsigned long long> d_counters;  // one work-queue counter per J/K launch
   hfg::DevBuf<double> d_D, d_Ds, d_Jacc, d_Kacc, d_J, d_K, d_tmp;
 
   std::map<std::tuple<double, double, double, int>, std::unique_ptr<hfg::Plan>> plans;

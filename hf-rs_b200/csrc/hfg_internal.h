@@ -30,6 +30,15 @@ struct PrimPair {
   double pad;
 };
 
+// Compact primitive-pair records read by the J/K kernels (structure of
+// arrays next to a float bound array): P - A = -bp * AB with bp = beta/p.
+struct __align__(32) PrimRec64 {
+  double p, inv_p, kp, bp;
+};
+struct __align__(16) PrimRec32 {
+  float p, inv_p, kp, bp;
+};
+
 // Work entry of one J/K launch: bra pair and the range of ket pairs
 // [k_lo, k_hi) (global pair indices, kets of one pair class).
 struct JKEntry {
@@ -42,9 +51,14 @@ struct JKLaunchArgs {
   int nentries;
   long long nwarps;
   const PairInfo* pairs;
-  const PrimPair* prims;
+  const PrimRec64* rec64;
+  const PrimRec32* rec32;
+  const float* pbound;  // primitive-pair bounds, sorted descending within each pair
   const double* boys64;
   const float* boys32;
+  const double* expt64;  // e^{-T0} per Boys grid row
+  const float* expt32;
+  unsigned long long* counter;  // work-queue counter of this launch (zeroed before it)
   const double* Dtot;  // n x n
   const double* Dspin; // nspin n x n
   double* Jacc;        // n x n

@@ -4,9 +4,9 @@
 
 namespace hfg {
 
-cudaError_t launch_jk(int la, int lb, int lc, int ld, int G, bool fp32, const JKLaunchArgs& a, cudaStream_t st) {
+cudaError_t launch_jk(int la, int lb, int lc, int ld, bool fp32, const JKLaunchArgs& a, cudaStream_t st) {
 #define HFG_CASE(A, B, C, D) \
-  if (la == A && lb == B && lc == C && ld == D) return launch_jk_##A##B##C##D(a, G, fp32, st);
+  if (la == A && lb == B && lc == C && ld == D) return launch_jk_##A##B##C##D(a, fp32, st);
   HFG_CASE(0, 0, 0, 0)
   HFG_CASE(1, 0, 0, 0)
   HFG_CASE(1, 0, 1, 0)
@@ -33,12 +33,14 @@ cudaError_t launch_jk(int la, int lb, int lc, int ld, int G, bool fp32, const JK
 }
 
 cudaError_t launch_schwarz(int la, int lb, const PairInfo* pairs, const PrimPair* prims, int first, int count,
-                           const double* boys, double* out, int prim_mode, cudaStream_t st) {
+                           const double* boys, const double* expt, double* out, int prim_mode, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
+  const int smem = (int)boys_smem_bytes<double>();
   const int block = 64, grid = (count + block - 1) / block;
 #define HFG_CASE(A, B)                                                                             \
   if (la == A && lb == B) {                                                                        \
-    schwarz_kernel<A, B><<<grid, block, 0, st>>>(pairs, prims, first, count, boys, out, prim_mode); \
+    cudaFuncSetAttribute(schwarz_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);             \
+    schwarz_kernel<A, B><<<grid, block, smem, st>>>(pairs, prims, first, count, boys, expt, out, prim_mode);   \
     return cudaGetLastError();                                                                     \
   }
   HFG_CASE(0, 0)
@@ -52,10 +54,12 @@ cudaError_t launch_schwarz(int la, int lb, const PairInfo* pairs, const PrimPair
 }
 
 cudaError_t launch_quartet(int la, int lb, int lc, int ld, const PairInfo* pairs, const PrimPair* prims,
-                           const double* boys, double* out, cudaStream_t st) {
+                           const double* boys, const double* expt, double* out, cudaStream_t st) {
+  const int smem = (int)boys_smem_bytes<double>();
 #define HFG_CASE(A, B, C, D)                                                    \
   if (la == A && lb == B && lc == C && ld == D) {                               \
-    quartet_kernel<A, B, C, D><<<1, 32, 0, st>>>(pairs, prims, boys, out);      \
+    cudaFuncSetAttribute(quartet_kernel<A, B, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); \
+    quartet_kernel<A, B, C, D><<<1, 32, smem, st>>>(pairs, prims, boys, expt, out);                  \
     return cudaGetLastError();                                                  \
   }
 #define HFG_KET(A, B) \

@@ -16,12 +16,16 @@
 //   K'[a,d] += 2 w Σ (ab|cd) D[b,c]      K'[b,d] += 2 w Σ (ab|cd) D[a,c]
 // which equals contract_jk's 8-permutation loop for symmetric densities.
 //
-// Work split: a warp takes one bra shell pair and up to 32/G ket pairs of
-// one pair class; a group of G lanes evaluates one shell quartet, its lanes
-// striding over the primitive quartets, then reduces its accumulators with
-// warp shuffles.  G is chosen per launch from the contraction lengths so that
-// heavily contracted quartets (cc-pVDZ oxygen 1s/2s: 81 primitive pairs)
-// spread over a whole warp while uncontracted ones take one lane each.
+// Work split: a warp takes one bra shell pair and up to 32 ket pairs of one
+// pair class, one shell quartet per lane.  Each lane keeps its ket
+// primitive pair in registers (outer loop) while the warp walks the bra
+// primitive pairs together (inner loop: every lane reads the same address,
+// one broadcast transaction).  Primitive pairs are sorted by their own
+// Cauchy-Schwarz bound, so primitive screening ends both loops early.
+// Blocks are persistent: each stages the Boys Taylor rows it needs in shared
+// memory once and then strides over the launch's warp tasks.  The J'[a,b]
+// contribution, common to the warp's bra pair, is reduced across the warp
+// before its atomics.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -47,42 +51,66 @@ __device__ __forceinline__ double comp_scale(int l, int i) {
 template <typename T> struct Prec;
 template <> struct Prec<double> {
   __device__ static const double* table(const JKLaunchArgs& a) { return a.boys64; }
+  __device__ static const double* expt(const JKLaunchArgs& a) { return a.expt64; }
 };
 template <> struct Prec<float> {
   __device__ static const float* table(const JKLaunchArgs& a) { return a.boys32; }
+  __device__ static const float* expt(const JKLaunchArgs& a) { return a.expt32; }
 };
 
-// One primitive quartet added into acc.  AC = A - C of the two pairs.
+template <typename T> __device__ __forceinline__ T rsqrt_t(T x);
+template <> __device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt(x); }
+template <> __device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
+
+// One primitive quartet added into acc: bra primitive pair (p, 1/p, kp,
+// P - A) and ket primitive pair (q, 1/q, kq, Q - C); AC = A - C.
 template <int LA, int LB, int LC, int LD, typename T>
-__device__ __forceinline__ void prim_quartet(T* __restrict__ acc, const PrimPair& P, const PrimPair& Q, T ACx, T ACy,
-                                             T ACz, const T* __restrict__ table) {
+__device__ __forceinline__ void prim_quartet(T* __restrict__ acc, T p, T inv_p, T kpp, T PAx, T PAy, T PAz, T q,
+                                             T inv_q, T kpq, T QCx, T QCy, T QCz, T ACx, T ACy, T ACz,
+                                             const T* __restrict__ sm) {
   using C = EriClass<LA, LB, LC, LD>;
   constexpr int L = C::L;
-  const T p = (T)P.p, q = (T)Q.p;
-  const T PAx = (T)P.PAx, PAy = (T)P.PAy, PAz = (T)P.PAz;
-  const T QCx = (T)Q.PAx, QCy = (T)Q.PAy, QCz = (T)Q.PAz;
   const T PQx = ACx + PAx - QCx, PQy = ACy + PAy - QCy, PQz = ACz + PAz - QCz;
   const T s = p + q;
-  T r;
-  if constexpr (sizeof(T) == 8) r = rsqrt(s); else r = rsqrtf(s);
+  const T r = rsqrt_t<T>(s);
   const T inv_s = r * r;
   const T pq_s = p * q * inv_s;
   const T tt = pq_s * (PQx * PQx + PQy * PQy + PQz * PQz);
   T F[L + 1];
-  boys_eval<L>(tt, table, F);
-  const T pref = (T)kTwoPiPow25 * (T)P.kp * (T)Q.kp * r;
+  boys_eval<L>(tt, sm, F);
+  const T pref = (T)kTwoPiPow25 * kpp * kpq * r;
 #pragma unroll
   for (int m = 0; m <= L; ++m) F[m] *= pref;
   const T qs = q * inv_s, ps = p * inv_s;
   C::prim(acc, F, PAx, PAy, PAz, -qs * PQx, -qs * PQy, -qs * PQz, QCx, QCy, QCz, ps * PQx, ps * PQy, ps * PQz,
-          (T)0.5 * (T)P.inv_p, (T)0.5 * (T)Q.inv_p, (T)0.5 * inv_s, qs, ps);
+          (T)0.5 * inv_p, (T)0.5 * inv_q, (T)0.5 * inv_s, qs, ps);
 }
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void prim_quartet_pp(double* __restrict__ acc, const PrimPair& P, const PrimPair& Q,
+                                                double ACx, double ACy, double ACz, const double* __restrict__ sm) {
+  prim_quartet<LA, LB, LC, LD, double>(acc, P.p, P.inv_p, P.kp, P.PAx, P.PAy, P.PAz, Q.p, Q.inv_p, Q.kp, Q.PAx,
+                                       Q.PAy, Q.PAz, ACx, ACy, ACz, sm);
+}
+
+template <typename T> struct RecOf;
+template <> struct RecOf<double> {
+  using type = PrimRec64;
+  __device__ static const PrimRec64* get(const JKLaunchArgs& a) { return a.rec64; }
+};
+template <> struct RecOf<float> {
+  using type = PrimRec32;
+  __device__ static const PrimRec32* get(const JKLaunchArgs& a) { return a.rec32; }
+};
 
 // Fused digestion of one scaled Cartesian block (w already includes deg and
 // the component scales).
+// Fused digestion of one scaled Cartesian block (w already includes deg and
+// the component scales), except J'[a,b] which the caller reduces across the
+// warp (jab receives this lane's sum over c,d).
 template <int LA, int LB, int LC, int LD>
 __device__ __forceinline__ void digest(const double* __restrict__ w, const PairInfo& bra, const PairInfo& ket,
-                                       const JKLaunchArgs& a) {
+                                       const JKLaunchArgs& a, double* __restrict__ jab) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   const int n = a.n;
   const int i0 = bra.ao_a, j0 = bra.ao_b, k0 = ket.ao_a, l0 = ket.ao_b;
@@ -97,14 +125,12 @@ __device__ __forceinline__ void digest(const double* __restrict__ w, const PairI
 #pragma unroll
       for (int j = 0; j < NB; ++j) dab[i * NB + j] = __ldg(a.Dtot + (size_t)(i0 + i) * n + j0 + j);
 #pragma unroll
-    for (int i = 0; i < NA; ++i)
+    for (int ij = 0; ij < NA * NB; ++ij) {
+      double s = 0.0;
 #pragma unroll
-      for (int j = 0; j < NB; ++j) {
-        double s = 0.0;
-#pragma unroll
-        for (int kl = 0; kl < NC * ND; ++kl) s += w[(i * NB + j) * NC * ND + kl] * dcd[kl];
-        atomicAdd(a.Jacc + (size_t)(i0 + i) * n + j0 + j, 4.0 * s);
-      }
+      for (int kl = 0; kl < NC * ND; ++kl) s += w[ij * NC * ND + kl] * dcd[kl];
+      jab[ij] = 4.0 * s;
+    }
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
@@ -195,86 +221,109 @@ __device__ __forceinline__ int find_entry(const long long* __restrict__ prefix, 
   return lo;
 }
 
-template <int LA, int LB, int LC, int LD, int G, typename T>
-__global__ void __launch_bounds__(128) jk_kernel(const JKLaunchArgs a) {
+// Warp tasks are handed out in chunks of kChunk consecutive tasks through
+// a per-launch atomic counter; consecutive tasks usually share a work entry,
+// so the entry lookup is a binary search once per chunk.
+constexpr int kChunk = 8;
+
+template <int LA, int LB, int LC, int LD, typename T>
+__global__ void __launch_bounds__(256, 3) jk_kernel(const JKLaunchArgs a) {
   using C = EriClass<LA, LB, LC, LD>;
-  constexpr int QPW = 32 / G;  // quartets per warp
-  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (warp >= a.nwarps) return;
+  constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  boys_stage<T, C::L>(sm, Prec<T>::table(a), Prec<T>::expt(a));
+  __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int e = find_entry(a.prefix, a.nentries, warp);
-  const JKEntry ent = a.entries[e];
-  const long long chunk = warp - a.prefix[e];
-  const int grp = lane / G, gl = lane % G;
-  const int kidx = ent.k_lo + (int)chunk * QPW + grp;
-  const bool active = kidx < ent.k_hi;
-  const PairInfo bra = a.pairs[ent.bra];
-  const PairInfo ket = a.pairs[active ? kidx : ent.k_lo];
+  for (;;) {
+    long long t0 = 0;
+    if (lane == 0) t0 = (long long)atomicAdd(a.counter, (unsigned long long)kChunk);
+    t0 = __shfl_sync(0xffffffffu, t0, 0);
+    if (t0 >= a.nwarps) break;
+    const long long t1 = t0 + kChunk < a.nwarps ? t0 + kChunk : a.nwarps;
+    int e = find_entry(a.prefix, a.nentries, t0);
+    long long next = a.prefix[e + 1];
+    for (long long warp = t0; warp < t1; ++warp) {
+      while (warp >= next) {
+        ++e;
+        next = a.prefix[e + 1];
+      }
+      const JKEntry ent = a.entries[e];
+      const int kidx = ent.k_lo + (int)(warp - a.prefix[e]) * 32 + lane;
+      const bool active = kidx < ent.k_hi;
+      const PairInfo bra = a.pairs[ent.bra];
+      const PairInfo ket = a.pairs[active ? kidx : ent.k_lo];
 
-  T acc[C::NACC];
+      T acc[C::NACC];
 #pragma unroll
-  for (int x = 0; x < C::NACC; ++x) acc[x] = (T)0;
+      for (int x = 0; x < C::NACC; ++x) acc[x] = (T)0;
 
-  if (active) {
-    const T ACx = (T)(bra.Ax - ket.Ax), ACy = (T)(bra.Ay - ket.Ay), ACz = (T)(bra.Az - ket.Az);
-    const PrimPair* __restrict__ bp = a.prims + bra.pp_off;
-    const PrimPair* __restrict__ kp = a.prims + ket.pp_off;
-    const int nb = bra.npp, nk = ket.npp;
-    const double eps = a.prim_eps;
-    if (G == 1) {
-      for (int ib = 0; ib < nb; ++ib) {
-        const PrimPair P = bp[ib];
-        if (P.bound * kp[0].bound < eps) break;
-        for (int ik = 0; ik < nk; ++ik) {
-          const PrimPair Q = kp[ik];
-          if (P.bound * Q.bound < eps) break;
-          prim_quartet<LA, LB, LC, LD, T>(acc, P, Q, ACx, ACy, ACz, Prec<T>::table(a));
+      if (active) {
+        using Rec = typename RecOf<T>::type;
+        const T ACx = (T)(bra.Ax - ket.Ax), ACy = (T)(bra.Ay - ket.Ay), ACz = (T)(bra.Az - ket.Az);
+        const T bABx = (T)bra.ABx, bABy = (T)bra.ABy, bABz = (T)bra.ABz;
+        const T kABx = (T)ket.ABx, kABy = (T)ket.ABy, kABz = (T)ket.ABz;
+        const Rec* __restrict__ br = RecOf<T>::get(a) + bra.pp_off;
+        const Rec* __restrict__ kr = RecOf<T>::get(a) + ket.pp_off;
+        const float* __restrict__ bb = a.pbound + bra.pp_off;
+        const float* __restrict__ kb = a.pbound + ket.pp_off;
+        const int nb = bra.npp, nk = ket.npp;
+        const double eps = a.prim_eps;
+        const double bmax = bb[0];
+        int nke = 0;  // ket primitive pairs that survive against the largest bra one
+        while (nke < nk && (double)kb[nke] * bmax >= eps) ++nke;
+        Rec Qn = kr[0];
+        for (int ik = 0; ik < nke; ++ik) {
+          const Rec Q = Qn;
+          if (ik + 1 < nke) Qn = kr[ik + 1];
+          const double qb = kb[ik];
+          const T QCx = -Q.bp * kABx, QCy = -Q.bp * kABy, QCz = -Q.bp * kABz;
+          Rec P = br[0];
+          for (int ib = 0; ib < nb; ++ib) {
+            const Rec Pn = br[ib + 1 < nb ? ib + 1 : ib];
+            if ((double)bb[ib] * qb < eps) break;
+            prim_quartet<LA, LB, LC, LD, T>(acc, P.p, P.inv_p, P.kp, -P.bp * bABx, -P.bp * bABy, -P.bp * bABz, Q.p,
+                                            Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
+            P = Pn;
+          }
         }
       }
-    } else {
-      const int total = nb * nk;
-      int ib = gl / nk, ik = gl - (gl / nk) * nk;
-      for (int t = gl; t < total; t += G) {
-        const PrimPair P = bp[ib];
-        const PrimPair Q = kp[ik];
-        if (P.bound * Q.bound >= eps) prim_quartet<LA, LB, LC, LD, T>(acc, P, Q, ACx, ACy, ACz, Prec<T>::table(a));
-        ik += G;
-        while (ik >= nk) {
-          ik -= nk;
-          ++ib;
-        }
+      double jab[NAB];
+      if (active) {
+        T out[C::NOUT];
+        C::hrr(acc, out, (T)bra.ABx, (T)bra.ABy, (T)bra.ABz, (T)ket.ABx, (T)ket.ABy, (T)ket.ABz);
+        double deg = 1.0;
+        if (bra.same) deg *= 0.5;
+        if (ket.same) deg *= 0.5;
+        if (kidx == ent.bra) deg *= 0.5;
+        double w[C::NOUT];
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+          for (int j = 0; j < NB; ++j)
+#pragma unroll
+            for (int k = 0; k < NC; ++k)
+#pragma unroll
+              for (int l = 0; l < ND; ++l) {
+                const int x = ((i * NB + j) * NC + k) * ND + l;
+                w[x] = (double)out[x] *
+                       (deg * comp_scale(LA, i) * comp_scale(LB, j) * comp_scale(LC, k) * comp_scale(LD, l));
+              }
+        digest<LA, LB, LC, LD>(w, bra, ket, a, jab);
+      } else {
+#pragma unroll
+        for (int x = 0; x < NAB; ++x) jab[x] = 0.0;
+      }
+      // J'[a,b]: the whole warp shares the bra pair
+#pragma unroll
+      for (int x = 0; x < NAB; ++x) {
+        double v = jab[x];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) atomicAdd(a.Jacc + (size_t)(bra.ao_a + x / NB) * a.n + bra.ao_b + x % NB, v);
       }
     }
   }
-  if (G > 1) {
-#pragma unroll
-    for (int x = 0; x < C::NACC; ++x) {
-#pragma unroll
-      for (int off = G / 2; off > 0; off >>= 1) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], off);
-    }
-  }
-  if (!active || gl != 0) return;
-
-  T out[C::NOUT];
-  C::hrr(acc, out, (T)bra.ABx, (T)bra.ABy, (T)bra.ABz, (T)ket.ABx, (T)ket.ABy, (T)ket.ABz);
-  double deg = 1.0;
-  if (bra.same) deg *= 0.5;
-  if (ket.same) deg *= 0.5;
-  if (kidx == ent.bra) deg *= 0.5;
-  constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-  double w[C::NOUT];
-#pragma unroll
-  for (int i = 0; i < NA; ++i)
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-#pragma unroll
-      for (int k = 0; k < NC; ++k)
-#pragma unroll
-        for (int l = 0; l < ND; ++l) {
-          const int x = ((i * NB + j) * NC + k) * ND + l;
-          w[x] = (double)out[x] * (deg * comp_scale(LA, i) * comp_scale(LB, j) * comp_scale(LC, k) * comp_scale(LD, l));
-        }
-  digest<LA, LB, LC, LD>(w, bra, ket, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -283,8 +332,13 @@ __global__ void __launch_bounds__(128) jk_kernel(const JKLaunchArgs a) {
 // block, square-rooted.
 template <int LA, int LB>
 __global__ void schwarz_kernel(const PairInfo* __restrict__ pairs, const PrimPair* __restrict__ prims, int first,
-                               int count, const double* __restrict__ boys, double* __restrict__ out, int prim_mode) {
+                               int count, const double* __restrict__ boys, const double* __restrict__ expt,
+                               double* __restrict__ out, int prim_mode) {
   using C = EriClass<LA, LB, LA, LB>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sm = reinterpret_cast<double*>(smem_raw);
+  boys_stage<double, C::L>(sm, boys, expt);
+  __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   // pair mode: t indexes shell pairs first + t; prim_mode: t indexes
@@ -298,7 +352,7 @@ __global__ void schwarz_kernel(const PairInfo* __restrict__ pairs, const PrimPai
   for (int x = 0; x < C::NACC; ++x) acc[x] = 0.0;
   for (int ib = 0; ib < np; ++ib)
     for (int ik = 0; ik < np; ++ik)
-      prim_quartet<LA, LB, LA, LB, double>(acc, prims[p0 + ib], prims[p0 + ik], 0.0, 0.0, 0.0, boys);
+      prim_quartet_pp<LA, LB, LA, LB>(acc, prims[p0 + ib], prims[p0 + ik], 0.0, 0.0, 0.0, sm);
   double blk[C::NOUT];
   C::hrr(acc, blk, owner.ABx, owner.ABy, owner.ABz, owner.ABx, owner.ABy, owner.ABz);
   constexpr int NA = ncart(LA), NB = ncart(LB), NAB = NA * NB;
@@ -317,16 +371,21 @@ __global__ void schwarz_kernel(const PairInfo* __restrict__ pairs, const PrimPai
 // One full Cartesian block (ab|cd) for the single-quartet entry point.
 template <int LA, int LB, int LC, int LD>
 __global__ void quartet_kernel(const PairInfo* __restrict__ pairs, const PrimPair* __restrict__ prims,
-                               const double* __restrict__ boys, double* __restrict__ out) {
+                               const double* __restrict__ boys, const double* __restrict__ expt,
+                               double* __restrict__ out) {
   using C = EriClass<LA, LB, LC, LD>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sm = reinterpret_cast<double*>(smem_raw);
+  boys_stage<double, C::L>(sm, boys, expt);
+  __syncthreads();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const PairInfo bra = pairs[0], ket = pairs[1];
   double acc[C::NACC];
   for (int x = 0; x < C::NACC; ++x) acc[x] = 0.0;
   for (int ib = 0; ib < bra.npp; ++ib)
     for (int ik = 0; ik < ket.npp; ++ik)
-      prim_quartet<LA, LB, LC, LD, double>(acc, prims[bra.pp_off + ib], prims[ket.pp_off + ik], bra.Ax - ket.Ax,
-                                           bra.Ay - ket.Ay, bra.Az - ket.Az, boys);
+      prim_quartet_pp<LA, LB, LC, LD>(acc, prims[bra.pp_off + ib], prims[ket.pp_off + ik], bra.Ax - ket.Ax,
+                                      bra.Ay - ket.Ay, bra.Az - ket.Az, sm);
   double blk[C::NOUT];
   C::hrr(acc, blk, bra.ABx, bra.ABy, bra.ABz, ket.ABx, ket.ABy, ket.ABz);
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);

@@ -88,6 +88,7 @@ def load_library():
     L.hfg_fock_rhf.argtypes = [VP, P(JKOptions), DP, DP, DP]
     L.hfg_fock_uhf.argtypes = [VP, P(JKOptions), DP, DP, DP, DP, DP]
     L.hfg_jk_last_stats.argtypes = [VP, P(JKStats)]
+    L.hfg_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, DP]
     _lib = L
     return L
 
@@ -97,6 +98,16 @@ def exported_functions():
     import re
     txt = open(HEADER).read()
     return sorted(set(re.findall(r"^\s*(?:int|void|const char\*)\s+(hfg_\w+)\s*\(", txt, re.M)))
+
+
+def fma_peak_tflops(device=0, fp32=False):
+    """Measured FP64 (or FP32) FMA-pipe peak of the device (hfg_fma_peak)."""
+    L = load_library()
+    out = ctypes.c_double()
+    rc = L.hfg_fma_peak(device, 1 if fp32 else 0, ctypes.byref(out))
+    if rc != 0:
+        raise HfgError(rc, "hfg_fma_peak failed")
+    return out.value
 
 
 class Context:
@@ -109,6 +120,8 @@ class Context:
         self._b = HfgBasis(basis.n, _dp(basis.center), _ip(basis.lxyz), _ip(basis.atom), _ip(basis.prim_off),
                            _dp(basis.exps), _dp(basis.coefs))
         h = VP()
+        if stream == 0:
+            raise HfgError(1, "pass a non-default CUDA stream (or None for a context-owned stream)")
         rc = self.lib.hfg_ctx_create(ctypes.byref(self._b), device, stream, ctypes.byref(h))
         self.h = h
         if rc != 0:

@@ -125,6 +125,11 @@ typedef struct {
 } hfg_jk_stats;
 int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* stats);
 
+/* Measured FMA-pipe peak of the device in TFLOP/s (FP64 when fp32 == 0):
+   independent FMA chains in registers on every SM.  The roofline
+   denominator of the ERI kernels, which are bound by these pipes. */
+int hfg_fma_peak(int device, int fp32, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif
