@@ -85,6 +85,7 @@ def load_library():
     L.hfg_shell_quartet.argtypes = [VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP]
     L.hfg_jk.argtypes = [VP, P(JKOptions), ctypes.c_int, DP, DP, DP, DP]
     L.hfg_jk_device.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
+    L.hfg_jk_device_noalloc.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
     L.hfg_fock_rhf.argtypes = [VP, P(JKOptions), DP, DP, DP]
     L.hfg_fock_uhf.argtypes = [VP, P(JKOptions), DP, DP, DP, DP, DP]
     L.hfg_jk_last_stats.argtypes = [VP, P(JKStats)]

@@ -106,6 +106,24 @@ int hfg_jk(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* P_tot
 int hfg_jk_device(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* d_P_total,
                   const double* d_P_spin, double* d_J, double* d_K);
 
+/*
+ * No counterpart in hf-rs.  As hfg_jk_device, but allocates no device
+ * memory at all, for callers that cannot allocate while they run (inside
+ * a CUDA stream capture, in latency-bound loops that cannot take
+ * cudaMalloc's device synchronisation, or under an allocator that owns all
+ * device memory).  The J'/K' accumulators and work-queue counters live in
+ * one 8 MiB device array that the library reserves when it is loaded, so
+ * (1 + nspin) * n^2 doubles must fit: n <= 724 (RHF), n <= 591 (UHF); larger
+ * systems return HFG_ERR_INVALID_INPUT.  The launch plan for `opts` must
+ * already exist on the context (one earlier hfg_jk or hfg_jk_device call
+ * with the same options builds it).  The first call on a device looks up
+ * the array's device address; make that first call before any stream
+ * capture.  All calls on a device share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller.
+ */
+int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* d_P_total,
+                          const double* d_P_spin, double* d_J, double* d_K);
+
 /* Stands in for build_fock_matrix (src/scf.rs:366-369): F = H + J - K/2. */
 int hfg_fock_rhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* P, double* F);
 
