@@ -42,6 +42,32 @@ class JKOptions(ctypes.Structure):
         return o
 
 
+class SCFOptions(ctypes.Structure):
+    _fields_ = [("natom", ctypes.c_int), ("positions", ctypes.POINTER(ctypes.c_double)),
+                ("charges", ctypes.POINTER(ctypes.c_double)), ("charge", ctypes.c_int),
+                ("multiplicity", ctypes.c_int), ("uhf", ctypes.c_int), ("spherical", ctypes.c_int),
+                ("max_iter", ctypes.c_int), ("energy_tol", ctypes.c_double), ("residual_tol", ctypes.c_double),
+                ("density_tol", ctypes.c_double), ("jk", JKOptions), ("refine_iters", ctypes.c_int),
+                ("diis_size", ctypes.c_int), ("verbose", ctypes.c_int)]
+
+
+class SCFResult(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("electronic", ctypes.c_double), ("nuclear", ctypes.c_double),
+                ("energy_before_refinement", ctypes.c_double), ("s2", ctypes.c_double),
+                ("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("n_mo", ctypes.c_int),
+                ("fock_builds_fp64", ctypes.c_int), ("fock_builds_mixed", ctypes.c_int), ("time_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def convergence_from_tol(tol):
+    """Residual and density tolerances hf-rs derives from an energy tolerance
+    (src/scf.rs:393-399)."""
+    import math
+    return tol, max(math.sqrt(tol) * 1e-2, 1e-11), min(max(math.sqrt(tol) * 0.1, 1e-12), 1e-10)
+
+
 class JKStats(ctypes.Structure):
     _fields_ = [("quartets_fp64", ctypes.c_double), ("quartets_fp32", ctypes.c_double),
                 ("prim_quartets_fp64", ctypes.c_double), ("prim_quartets_fp32", ctypes.c_double),
@@ -90,6 +116,8 @@ def load_library():
     L.hfg_fock_uhf.argtypes = [VP, P(JKOptions), DP, DP, DP, DP, DP]
     L.hfg_jk_last_stats.argtypes = [VP, P(JKStats)]
     L.hfg_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, DP]
+    L.hfg_scf_opts_default.argtypes = [P(SCFOptions)]
+    L.hfg_scf.argtypes = [VP, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     _lib = L
     return L
 
@@ -195,6 +223,41 @@ class Context:
                                           _dp(np.ascontiguousarray(Pa)), _dp(np.ascontiguousarray(Pb)),
                                           _dp(Fa), _dp(Fb)))
         return Fa, Fb
+
+    def scf(self, charge=0, multiplicity=1, uhf=False, spherical=False, tol=1e-10, max_iter=100, jk=None,
+            refine_iters=2, verbose=False, want=("P", "F")):
+        """Device SCF (hfg_scf) for the context's molecule; returns a dict."""
+        b = self.basis
+        o = SCFOptions()
+        self.lib.hfg_scf_opts_default(ctypes.byref(o))
+        pos = np.ascontiguousarray(b.positions())
+        chg = np.ascontiguousarray(b.nuclear_charges())
+        o.natom = len(chg)
+        o.positions = _dp(pos)
+        o.charges = _dp(chg)
+        o.charge, o.multiplicity, o.uhf, o.spherical = charge, multiplicity, int(uhf), int(spherical)
+        o.max_iter = max_iter
+        o.energy_tol, o.residual_tol, o.density_tol = convergence_from_tol(tol)
+        o.jk = jk or JKOptions.make()
+        o.refine_iters = refine_iters
+        o.verbose = int(verbose)
+        n = self.n
+        ns = 2 if uhf else 1
+        P = np.zeros((ns, n, n)) if "P" in want else None
+        F = np.zeros((ns, n, n)) if "F" in want else None
+        C = np.zeros((ns, n, n)) if "C" in want else None
+        eps = np.zeros((ns, n)) if "eps" in want else None
+        r = SCFResult()
+        rc = self.lib.hfg_scf(self.h, ctypes.byref(o), ctypes.byref(r), _dp(P) if P is not None else None,
+                              _dp(F) if F is not None else None, _dp(C) if C is not None else None,
+                              _dp(eps) if eps is not None else None)
+        if rc not in (0, 3):
+            self._check(rc)
+        out = r.as_dict()
+        m = r.n_mo
+        out.update({"P": P, "F": F, "C": None if C is None else C.reshape(ns, -1)[:, :n * m].reshape(ns, n, m),
+                    "eps": None if eps is None else eps[:, :m], "status": rc})
+        return out
 
     def last_stats(self):
         s = JKStats()

@@ -143,6 +143,52 @@ typedef struct {
 } hfg_jk_stats;
 int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* stats);
 
+/* Options of hfg_scf: nuclei, electrons, AO space and convergence controls of
+   run_scf_in_space_with_convergence / run_uhf_in_space_with_convergence
+   (src/scf.rs:410, :691; RhfConvergence src/scf.rs:400-407). */
+typedef struct {
+  int natom;
+  const double* positions; /* [natom][3] bohr */
+  const double* charges;   /* [natom] nuclear charges */
+  int charge;              /* molecular charge */
+  int multiplicity;        /* 2S + 1 */
+  int uhf;                 /* 0: RHF, 1: UHF */
+  int spherical;           /* 1: real spherical AO space (BasisKind::Spherical, src/ao.rs:14-27) */
+  int max_iter;
+  double energy_tol, residual_tol, density_tol;
+  hfg_jk_opts jk;          /* J/K options; HFG_MIXED runs FP32 quartets until converged,
+                              then FP64 iterations (refine_iters at least) to convergence */
+  int refine_iters;
+  int diis_size;           /* CDIIS subspace (hf-rs: 8, src/scf.rs:479) */
+  int verbose;             /* iteration table on stderr */
+} hfg_scf_opts;
+
+typedef struct {
+  double energy, electronic, nuclear;
+  double energy_before_refinement; /* HFG_MIXED: energy when the mixed phase converged */
+  double s2;                       /* UHF <S^2> */
+  int iterations, converged, n_mo;
+  int fock_builds_fp64, fock_builds_mixed;
+  double time_ms;
+} hfg_scf_result;
+
+/* Defaults: RHF singlet, 100 iterations, tolerances derived from 1e-10 as
+   run_scf_in_space does (src/scf.rs:393-399), FP64 J/K, 2 refinement
+   iterations, CDIIS(8). */
+void hfg_scf_opts_default(hfg_scf_opts* opts);
+
+/*
+ * Stands in for run_scf_in_space_with_convergence (src/scf.rs:410-627) and
+ * run_uhf_in_space_with_convergence (src/scf.rs:691-979) with CDIIS: a
+ * direct SCF whose one-electron integrals, Fock builds, DIIS and
+ * diagonalisations all run on the device.  Initial guess: core Hamiltonian.
+ * Optional outputs (NULL to skip), row-major: P and F (nspin x n x n),
+ * C (nspin x n x n_mo, Cartesian rows), orbital energies (nspin x n_mo).
+ * Returns HFG_ERR_SCF if not converged within max_iter (results still set).
+ */
+int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* opts, hfg_scf_result* result, double* P, double* F, double* C,
+            double* eps);
+
 /* Measured FMA-pipe peak of the device in TFLOP/s (FP64 when fp32 == 0):
    independent FMA chains in registers on every SM.  The roofline
    denominator of the ERI kernels, which are bound by these pipes. */
