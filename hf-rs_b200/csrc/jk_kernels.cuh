@@ -105,63 +105,76 @@ template <> struct RecOf<float> {
 
 // Fused digestion of one scaled Cartesian block (w already includes deg and
 // the component scales).
+// Density blocks needed by the digestion of one quartet (loaded before the
+// primitive loop so their latency overlaps the integral work).
+template <int LA, int LB, int LC, int LD, int NS>
+struct DBlocks {
+  static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  double cd[NC * ND], ab[NA * NB];
+  double bd[NS][NB * ND], ad[NS][NA * ND], bc[NS][NB * NC], ac[NS][NA * NC];
+  __device__ __forceinline__ void load(const PairInfo& bra, const PairInfo& ket, const JKLaunchArgs& a) {
+    const int n = a.n;
+    const int i0 = bra.ao_a, j0 = bra.ao_b, k0 = ket.ao_a, l0 = ket.ao_b;
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) cd[k * ND + l] = __ldg(a.Dtot + (size_t)(k0 + k) * n + l0 + l);
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int j = 0; j < NB; ++j) ab[i * NB + j] = __ldg(a.Dtot + (size_t)(i0 + i) * n + j0 + j);
+#pragma unroll
+    for (int sp = 0; sp < NS; ++sp) {
+      const double* D = a.Dspin + (size_t)sp * n * n;
+#pragma unroll
+      for (int j = 0; j < NB; ++j)
+#pragma unroll
+        for (int l = 0; l < ND; ++l) bd[sp][j * ND + l] = __ldg(D + (size_t)(j0 + j) * n + l0 + l);
+#pragma unroll
+      for (int i = 0; i < NA; ++i)
+#pragma unroll
+        for (int l = 0; l < ND; ++l) ad[sp][i * ND + l] = __ldg(D + (size_t)(i0 + i) * n + l0 + l);
+#pragma unroll
+      for (int j = 0; j < NB; ++j)
+#pragma unroll
+        for (int k = 0; k < NC; ++k) bc[sp][j * NC + k] = __ldg(D + (size_t)(j0 + j) * n + k0 + k);
+#pragma unroll
+      for (int i = 0; i < NA; ++i)
+#pragma unroll
+        for (int k = 0; k < NC; ++k) ac[sp][i * NC + k] = __ldg(D + (size_t)(i0 + i) * n + k0 + k);
+    }
+  }
+};
+
 // Fused digestion of one scaled Cartesian block (w already includes deg and
 // the component scales), except J'[a,b] which the caller reduces across the
 // warp (jab receives this lane's sum over c,d).
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, int NS>
 __device__ __forceinline__ void digest(const double* __restrict__ w, const PairInfo& bra, const PairInfo& ket,
-                                       const JKLaunchArgs& a, double* __restrict__ jab) {
+                                       const JKLaunchArgs& a, const DBlocks<LA, LB, LC, LD, NS>& d,
+                                       double* __restrict__ jab) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   const int n = a.n;
   const int i0 = bra.ao_a, j0 = bra.ao_b, k0 = ket.ao_a, l0 = ket.ao_b;
-  {
-    double dcd[NC * ND], dab[NA * NB];
 #pragma unroll
-    for (int k = 0; k < NC; ++k)
+  for (int ij = 0; ij < NA * NB; ++ij) {
+    double s = 0.0;
 #pragma unroll
-      for (int l = 0; l < ND; ++l) dcd[k * ND + l] = __ldg(a.Dtot + (size_t)(k0 + k) * n + l0 + l);
+    for (int kl = 0; kl < NC * ND; ++kl) s += w[ij * NC * ND + kl] * d.cd[kl];
+    jab[ij] = 4.0 * s;
+  }
 #pragma unroll
-    for (int i = 0; i < NA; ++i)
+  for (int k = 0; k < NC; ++k)
 #pragma unroll
-      for (int j = 0; j < NB; ++j) dab[i * NB + j] = __ldg(a.Dtot + (size_t)(i0 + i) * n + j0 + j);
-#pragma unroll
-    for (int ij = 0; ij < NA * NB; ++ij) {
+    for (int l = 0; l < ND; ++l) {
       double s = 0.0;
 #pragma unroll
-      for (int kl = 0; kl < NC * ND; ++kl) s += w[ij * NC * ND + kl] * dcd[kl];
-      jab[ij] = 4.0 * s;
+      for (int ij = 0; ij < NA * NB; ++ij) s += w[ij * NC * ND + k * ND + l] * d.ab[ij];
+      atomicAdd(a.Jacc + (size_t)(k0 + k) * n + l0 + l, 4.0 * s);
     }
 #pragma unroll
-    for (int k = 0; k < NC; ++k)
-#pragma unroll
-      for (int l = 0; l < ND; ++l) {
-        double s = 0.0;
-#pragma unroll
-        for (int ij = 0; ij < NA * NB; ++ij) s += w[ij * NC * ND + k * ND + l] * dab[ij];
-        atomicAdd(a.Jacc + (size_t)(k0 + k) * n + l0 + l, 4.0 * s);
-      }
-  }
-  for (int sp = 0; sp < a.nspin; ++sp) {
-    const double* D = a.Dspin + (size_t)sp * n * n;
+  for (int sp = 0; sp < NS; ++sp) {
     double* K = a.Kacc + (size_t)sp * n * n;
-    double dbd[NB * ND], dad[NA * ND], dbc[NB * NC], dac[NA * NC];
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-#pragma unroll
-      for (int l = 0; l < ND; ++l) dbd[j * ND + l] = __ldg(D + (size_t)(j0 + j) * n + l0 + l);
-#pragma unroll
-    for (int i = 0; i < NA; ++i)
-#pragma unroll
-      for (int l = 0; l < ND; ++l) dad[i * ND + l] = __ldg(D + (size_t)(i0 + i) * n + l0 + l);
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-#pragma unroll
-      for (int k = 0; k < NC; ++k) dbc[j * NC + k] = __ldg(D + (size_t)(j0 + j) * n + k0 + k);
-#pragma unroll
-    for (int i = 0; i < NA; ++i)
-#pragma unroll
-      for (int k = 0; k < NC; ++k) dac[i * NC + k] = __ldg(D + (size_t)(i0 + i) * n + k0 + k);
-    // K'[a,c] += 2 Σ_{b,d} w D[b,d]
 #pragma unroll
     for (int i = 0; i < NA; ++i)
 #pragma unroll
@@ -170,10 +183,9 @@ __device__ __forceinline__ void digest(const double* __restrict__ w, const PairI
 #pragma unroll
         for (int j = 0; j < NB; ++j)
 #pragma unroll
-          for (int l = 0; l < ND; ++l) s += w[((i * NB + j) * NC + k) * ND + l] * dbd[j * ND + l];
+          for (int l = 0; l < ND; ++l) s += w[((i * NB + j) * NC + k) * ND + l] * d.bd[sp][j * ND + l];
         atomicAdd(K + (size_t)(i0 + i) * n + k0 + k, 2.0 * s);
       }
-    // K'[b,c] += 2 Σ_{a,d} w D[a,d]
 #pragma unroll
     for (int j = 0; j < NB; ++j)
 #pragma unroll
@@ -182,10 +194,9 @@ __device__ __forceinline__ void digest(const double* __restrict__ w, const PairI
 #pragma unroll
         for (int i = 0; i < NA; ++i)
 #pragma unroll
-          for (int l = 0; l < ND; ++l) s += w[((i * NB + j) * NC + k) * ND + l] * dad[i * ND + l];
+          for (int l = 0; l < ND; ++l) s += w[((i * NB + j) * NC + k) * ND + l] * d.ad[sp][i * ND + l];
         atomicAdd(K + (size_t)(j0 + j) * n + k0 + k, 2.0 * s);
       }
-    // K'[a,d] += 2 Σ_{b,c} w D[b,c]
 #pragma unroll
     for (int i = 0; i < NA; ++i)
 #pragma unroll
@@ -194,10 +205,9 @@ __device__ __forceinline__ void digest(const double* __restrict__ w, const PairI
 #pragma unroll
         for (int j = 0; j < NB; ++j)
 #pragma unroll
-          for (int k = 0; k < NC; ++k) s += w[((i * NB + j) * NC + k) * ND + l] * dbc[j * NC + k];
+          for (int k = 0; k < NC; ++k) s += w[((i * NB + j) * NC + k) * ND + l] * d.bc[sp][j * NC + k];
         atomicAdd(K + (size_t)(i0 + i) * n + l0 + l, 2.0 * s);
       }
-    // K'[b,d] += 2 Σ_{a,c} w D[a,c]
 #pragma unroll
     for (int j = 0; j < NB; ++j)
 #pragma unroll
@@ -206,7 +216,7 @@ __device__ __forceinline__ void digest(const double* __restrict__ w, const PairI
 #pragma unroll
         for (int i = 0; i < NA; ++i)
 #pragma unroll
-          for (int k = 0; k < NC; ++k) s += w[((i * NB + j) * NC + k) * ND + l] * dac[i * NC + k];
+          for (int k = 0; k < NC; ++k) s += w[((i * NB + j) * NC + k) * ND + l] * d.ac[sp][i * NC + k];
         atomicAdd(K + (size_t)(j0 + j) * n + l0 + l, 2.0 * s);
       }
   }
@@ -226,8 +236,13 @@ __device__ __forceinline__ int find_entry(const long long* __restrict__ prefix, 
 // so the entry lookup is a binary search once per chunk.
 constexpr int kChunk = 8;
 
-template <int LA, int LB, int LC, int LD, typename T>
-__global__ void __launch_bounds__(256, 3) jk_kernel(const JKLaunchArgs a) {
+// Resident blocks per SM the register allocation is tuned for.
+#ifndef HFG_JK_MIN_BLOCKS
+#define HFG_JK_MIN_BLOCKS 2
+#endif
+
+template <int LA, int LB, int LC, int LD, typename T, int NS>
+__global__ void __launch_bounds__(256, HFG_JK_MIN_BLOCKS) jk_kernel(const JKLaunchArgs a) {
   using C = EriClass<LA, LB, LC, LD>;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -253,6 +268,10 @@ __global__ void __launch_bounds__(256, 3) jk_kernel(const JKLaunchArgs a) {
       const bool active = kidx < ent.k_hi;
       const PairInfo bra = a.pairs[ent.bra];
       const PairInfo ket = a.pairs[active ? kidx : ent.k_lo];
+      // the next task usually continues this entry: touch its ket pair now
+      if (warp + 1 < t1 && kidx + 32 < ent.k_hi) (void)__ldg(&a.pairs[kidx + 32].pp_off);
+      DBlocks<LA, LB, LC, LD, NS> dblk;
+      if (active) dblk.load(bra, ket, a);
 
       T acc[C::NACC];
 #pragma unroll
@@ -270,8 +289,16 @@ __global__ void __launch_bounds__(256, 3) jk_kernel(const JKLaunchArgs a) {
         const int nb = bra.npp, nk = ket.npp;
         const double eps = a.prim_eps;
         const double bmax = bb[0];
-        int nke = 0;  // ket primitive pairs that survive against the largest bra one
-        while (nke < nk && (double)kb[nke] * bmax >= eps) ++nke;
+        // ket primitive pairs that survive against the largest bra one
+        // (bounds sorted descending: binary search)
+        int nke = 0;
+        {
+          int hi = nk;
+          while (nke < hi) {
+            const int mid = (nke + hi) >> 1;
+            if ((double)kb[mid] * bmax >= eps) nke = mid + 1; else hi = mid;
+          }
+        }
         Rec Qn = kr[0];
         for (int ik = 0; ik < nke; ++ik) {
           const Rec Q = Qn;
@@ -309,7 +336,7 @@ __global__ void __launch_bounds__(256, 3) jk_kernel(const JKLaunchArgs a) {
                 w[x] = (double)out[x] *
                        (deg * comp_scale(LA, i) * comp_scale(LB, j) * comp_scale(LC, k) * comp_scale(LD, l));
               }
-        digest<LA, LB, LC, LD>(w, bra, ket, a, jab);
+        digest<LA, LB, LC, LD, NS>(w, bra, ket, a, dblk, jab);
       } else {
 #pragma unroll
         for (int x = 0; x < NAB; ++x) jab[x] = 0.0;
