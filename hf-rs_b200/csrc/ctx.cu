@@ -54,7 +54,7 @@ static double wmd_flops(int la, int lb, int lc, int ld) {
 // Boys grid values F_0..F_{kBoysCols-1} at T = idx * 0.05, by the series at
 // the highest tabulated order (47) and downward recursion, as hf-rs builds
 // its table (src/integrals.rs:27-57).
-static const std::vector<double>& boys_table_host() {
+const std::vector<double>& boys_table_host() {
   static std::vector<double> table;
   static std::once_flag once;
   std::call_once(once, [] {
@@ -104,7 +104,7 @@ static double comp_scale_host(const std::array<int, 3>& l) {
 // Groups the Cartesian functions into shells with the semantics of hf-rs's
 // shell_ranges (src/ao.rs:133-164) and recovers the shell contraction
 // coefficients (component coefficient / component scale).
-static int build_shells(hfg_ctx* ctx, const hfg_basis* b) {
+int build_shell_list(hfg_ctx* ctx, const hfg_basis* b, int lmax) {
   if (!b || b->n <= 0 || !b->center || !b->lxyz || !b->atom || !b->prim_off || !b->exps || !b->coefs)
     return set_error(ctx, HFG_ERR_INVALID_INPUT, "empty or incomplete basis description");
   const int n = b->n;
@@ -115,7 +115,7 @@ static int build_shells(hfg_ctx* ctx, const hfg_basis* b) {
     const int* l0 = b->lxyz + 3 * start;
     const int l = l0[0] + l0[1] + l0[2];
     if (l < 0 || l > 7) return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid angular momentum");
-    if (l > kLMax) return set_error(ctx, HFG_ERR_UNSUPPORTED, "angular momentum above d is not built into the kernels");
+    if (l > lmax) return set_error(ctx, HFG_ERR_UNSUPPORTED, "angular momentum not built into the kernels");
     const int cnt = ncart(l);
     if (start + cnt > n) return set_error(ctx, HFG_ERR_INVALID_INPUT, "incomplete Cartesian shell");
     const int K = b->prim_off[start + 1] - b->prim_off[start];
@@ -167,7 +167,7 @@ static int build_shells(hfg_ctx* ctx, const hfg_basis* b) {
 }
 
 // Oriented pair (la >= lb, Ka >= Kb on ties) with its primitive pairs.
-static void make_pair(const hfg_ctx* ctx, int a, int b, PairInfo& pi, std::vector<PrimPair>& pp, int owner) {
+void make_pair(const hfg_ctx* ctx, int a, int b, PairInfo& pi, std::vector<PrimPair>& pp, int owner) {
   const Shell& A = ctx->shells[a];
   const Shell& B = ctx->shells[b];
   pi.Ax = A.c[0];
@@ -600,7 +600,7 @@ int hfg_ctx_create(const hfg_basis* basis, int device, void* stream, hfg_ctx** o
       ctx->own_stream = true;
     }
   }
-  if (rc == HFG_OK) rc = build_shells(ctx.get(), basis);
+  if (rc == HFG_OK) rc = build_shell_list(ctx.get(), basis, kLMax);
   if (rc == HFG_OK) {
     const auto& t = boys_table_host();
     std::vector<float> tf(t.begin(), t.end());

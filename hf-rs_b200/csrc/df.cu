@@ -1,0 +1,426 @@
+// Density fitting: DfTensor::build and coulomb_exchange_rhf on the device.
+//
+// Stands in for hf-rs's DfTensor::build / build_in_space (src/df.rs:89-127)
+// in the Cartesian auxiliary space and coulomb_exchange_rhf
+// (src/df.rs:133-174):
+//   M = (P|Q), X = canonical_orthogonalizer(M, cutoff) (src/df.rs:16-28),
+//   B = X^T (P|mn) over unique AO pairs m >= n,
+//   J = sum_Q (B_Q . P) B_Q,  K = 2 sum_Q (B_Q C_occ)(B_Q C_occ)^T.
+// Differences of layout, not of arithmetic: B is kept only for the AO pairs
+// of shell pairs whose Schwarz bound exceeds `pair_threshold` (0 keeps all,
+// as hf-rs does), and may be stored in FP32 or BF16.  J uses two GEMVs on
+// the packed B; K runs chunks of auxiliary functions through two GEMMs on
+// dense unpacked blocks (FP64, TF32 or BF16 tensor-core GEMMs with FP32
+// accumulation, summed into FP64).
+#include <cublas_v2.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <vector>
+
+#include "df_internal.h"
+#include "hfg_ctx.h"
+
+using namespace hfg;
+
+struct hfg_df {
+  hfg_ctx* ctx = nullptr;
+  int n = 0, naux = 0, rank = 0;
+  long long ncol = 0;
+  int storage = HFG_DF_FP64;
+  DevBuf<double> B64;
+  DevBuf<float> B32;
+  DevBuf<__nv_bfloat16> B16;
+  DevBuf<int2> colmn;
+  DevBuf<double> metric;  // kept for inspection (naux x naux)
+  cublasHandle_t blas = nullptr;
+  DevBuf<double> P, pvec, gam, jcol, Cd, J, K, T64;
+  DevBuf<float> gam32, jcol32, pvec32, Kf, Tf, Cf;
+  DevBuf<__nv_bfloat16> Cb, Tb;
+  DevBuf<unsigned char> dense;
+  ~hfg_df() {
+    if (blas) cublasDestroy(blas);
+  }
+};
+
+namespace {
+
+int gemm_ex(hfg_ctx* ctx, cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+            const void* A, cudaDataType ta_t, int lda, const void* B, cudaDataType tb_t, int ldb, float beta,
+            float* C, int ldc, cublasComputeType_t ct) {
+  const float alpha = 1.0f;
+  const cublasStatus_t s =
+      cublasGemmEx(h, ta, tb, m, n, k, &alpha, A, ta_t, lda, B, tb_t, ldb, &beta, C, CUDA_R_32F, ldc, ct,
+                   CUBLAS_GEMM_DEFAULT);
+  return s == CUBLAS_STATUS_SUCCESS ? HFG_OK : set_error(ctx, HFG_ERR_CUDA, "cublasGemmEx failed");
+}
+
+}  // namespace
+
+extern "C" {
+
+int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, double pair_threshold, int storage,
+                 hfg_df** out) {
+  if (!ctx || !aux || !out) return HFG_ERR_INVALID_INPUT;
+  *out = nullptr;
+  if (!(metric_cutoff > 0) || !std::isfinite(metric_cutoff))
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "DF metric cutoff must be finite and positive");
+  if (storage < HFG_DF_FP64 || storage > HFG_DF_BF16) return set_error(ctx, HFG_ERR_INVALID_INPUT, "storage");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  auto df = std::make_unique<hfg_df>();
+  df->ctx = ctx;
+  df->n = ctx->n;
+  df->storage = storage;
+  cudaStream_t st = ctx->stream;
+  int rc = HFG_OK;
+#define CK(call)                         \
+  do {                                   \
+    rc = cuda_check(ctx, (call), #call); \
+    if (rc != HFG_OK) return rc;         \
+  } while (0)
+  // auxiliary shells and their unit-partner "pairs"
+  hfg_ctx auxc;
+  rc = build_shell_list(&auxc, aux, 4);
+  if (rc != HFG_OK) return set_error(ctx, rc, "auxiliary basis: " + auxc.err);
+  const int naux = auxc.n;
+  df->naux = naux;
+  std::vector<PairInfo> upairs(auxc.shells.size());
+  std::vector<PrimPair> uprims;
+  for (size_t s = 0; s < auxc.shells.size(); ++s) {
+    const Shell& sh = auxc.shells[s];
+    PairInfo& pi = upairs[s];
+    pi = PairInfo{};
+    pi.Ax = sh.c[0];
+    pi.Ay = sh.c[1];
+    pi.Az = sh.c[2];
+    pi.ao_a = sh.ao;
+    pi.pp_off = (int)uprims.size();
+    pi.npp = sh.K;
+    for (int q = 0; q < sh.K; ++q) {
+      PrimPair p{};
+      p.p = auxc.exps[sh.prim_off + q];
+      p.inv_p = 1.0 / p.p;
+      p.kp = auxc.coefs[sh.prim_off + q] * p.inv_p;  // unit partner: coefficient 1, exp(0) = 1
+      uprims.push_back(p);
+    }
+  }
+  DevBuf<PairInfo> dup;
+  DevBuf<PrimPair> dupr;
+  CK(dup.alloc(upairs.size()));
+  CK(dupr.alloc(uprims.size()));
+  CK(cudaMemcpyAsync(dup.p, upairs.data(), upairs.size() * sizeof(PairInfo), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dupr.p, uprims.data(), uprims.size() * sizeof(PrimPair), cudaMemcpyHostToDevice, st));
+  std::map<int, std::vector<int>> aux_by_l;
+  for (size_t s = 0; s < auxc.shells.size(); ++s) aux_by_l[auxc.shells[s].l].push_back((int)s);
+  std::map<int, DevBuf<int>> aux_idx;
+  for (auto& kv : aux_by_l) {
+    CK(aux_idx[kv.first].alloc(kv.second.size()));
+    CK(cudaMemcpyAsync(aux_idx[kv.first].p, kv.second.data(), kv.second.size() * 4, cudaMemcpyHostToDevice, st));
+  }
+
+  // metric (P|Q): bra and ket both unit-paired auxiliary shells
+  CK(df->metric.alloc((size_t)naux * naux));
+  for (auto& bk : aux_by_l) {
+    std::vector<long long> cols;
+    for (int s : bk.second) cols.push_back(auxc.shells[s].ao);
+    DevBuf<long long> dcols;
+    CK(dcols.alloc(cols.size()));
+    CK(cudaMemcpyAsync(dcols.p, cols.data(), cols.size() * 8, cudaMemcpyHostToDevice, st));
+    for (auto& kk : aux_by_l) {
+      Df3cArgs a{dup.p, dupr.p, aux_idx[bk.first].p, dcols.p, (int)bk.second.size(), dup.p, dupr.p,
+                 aux_idx[kk.first].p, (int)kk.second.size(), ctx->d_boys64.p, ctx->d_expt64.p, df->metric.p, naux};
+      CK(launch_df3c(bk.first, 0, kk.first, a, st));
+    }
+    CK(cudaStreamSynchronize(st));
+  }
+  // canonical orthogonaliser of the metric (cutoff on its eigenvalues)
+  cusolverDnHandle_t solver = nullptr;
+  if (cusolverDnCreate(&solver) != CUSOLVER_STATUS_SUCCESS) return set_error(ctx, HFG_ERR_CUDA, "cusolver");
+  cusolverDnSetStream(solver, st);
+  DevBuf<double> V, w, work;
+  DevBuf<int> info;
+  CK(V.alloc((size_t)naux * naux));
+  CK(w.alloc(naux));
+  CK(info.alloc(1));
+  CK(cudaMemcpyAsync(V.p, df->metric.p, (size_t)naux * naux * 8, cudaMemcpyDeviceToDevice, st));
+  int lwork = 0;
+  cusolverDnDsyevd_bufferSize(solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, naux, V.p, naux, w.p, &lwork);
+  CK(work.alloc(lwork));
+  if (cusolverDnDsyevd(solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, naux, V.p, naux, w.p, work.p, lwork,
+                       info.p) != CUSOLVER_STATUS_SUCCESS) {
+    cusolverDnDestroy(solver);
+    return set_error(ctx, HFG_ERR_CUDA, "metric eigendecomposition failed");
+  }
+  std::vector<double> wh(naux);
+  CK(cudaMemcpyAsync(wh.data(), w.p, naux * 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  cusolverDnDestroy(solver);
+  if (wh[0] < -metric_cutoff) return set_error(ctx, HFG_ERR_INTEGRAL, "DF metric has a negative eigenvalue");
+  int first = 0;
+  while (first < naux && wh[first] < metric_cutoff) ++first;
+  const int rank = naux - first;
+  if (rank <= 0) return set_error(ctx, HFG_ERR_INTEGRAL, "DF metric has zero retained rank");
+  df->rank = rank;
+  // Xm = V[:, first:] diag(w^-1/2), column-major naux x rank
+  {
+    std::vector<double> Vh((size_t)naux * naux);
+    CK(cudaMemcpyAsync(Vh.data(), V.p, Vh.size() * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int c = 0; c < rank; ++c) {
+      const double sc = 1.0 / std::sqrt(wh[first + c]);
+      for (int r = 0; r < naux; ++r) Vh[(size_t)c * naux + r] = Vh[(size_t)(first + c) * naux + r] * sc;
+    }
+    CK(cudaMemcpyAsync(V.p, Vh.data(), (size_t)naux * rank * 8, cudaMemcpyHostToDevice, st));
+  }
+
+  // significant orbital shell pairs and their unique AO-pair columns
+  std::map<std::pair<int, int>, std::vector<int>> bra_by_class;
+  std::map<std::pair<int, int>, std::vector<long long>> col_by_class;
+  std::vector<int2> colmn;
+  long long ncol = 0;
+  for (size_t i = 0; i < ctx->h_pairs.size(); ++i) {
+    if (!(ctx->sorted_Q[i] > pair_threshold)) continue;
+    const PairInfo& pi = ctx->h_pairs[i];
+    const PairClass& c = ctx->classes[pi.cls];
+    const int na = (c.la + 1) * (c.la + 2) / 2, nb = (c.lb + 1) * (c.lb + 2) / 2;
+    bra_by_class[{c.la, c.lb}].push_back((int)i);
+    col_by_class[{c.la, c.lb}].push_back(ncol);
+    for (int a = 0; a < na; ++a)
+      for (int b = 0; b < nb; ++b) {
+        if (pi.same && b > a) continue;
+        colmn.push_back(make_int2(pi.ao_a + a, pi.ao_b + b));
+      }
+    ncol += pi.same ? na * (na + 1) / 2 : na * nb;
+  }
+  df->ncol = ncol;
+  CK(df->colmn.alloc(ncol));
+  CK(cudaMemcpyAsync(df->colmn.p, colmn.data(), ncol * sizeof(int2), cudaMemcpyHostToDevice, st));
+  // (P|mn) for all columns (rows = auxiliary functions), then B = Xm^T (P|mn)
+  DevBuf<double> T3;
+  CK(T3.alloc((size_t)naux * ncol));
+  for (auto& bc : bra_by_class) {
+    DevBuf<int> bidx;
+    DevBuf<long long> bcol;
+    CK(bidx.alloc(bc.second.size()));
+    CK(bcol.alloc(bc.second.size()));
+    CK(cudaMemcpyAsync(bidx.p, bc.second.data(), bc.second.size() * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(bcol.p, col_by_class[bc.first].data(), bc.second.size() * 8, cudaMemcpyHostToDevice, st));
+    for (auto& kk : aux_by_l) {
+      Df3cArgs a{ctx->d_pairs.p, ctx->d_prims.p, bidx.p, bcol.p, (int)bc.second.size(), dup.p, dupr.p,
+                 aux_idx[kk.first].p, (int)kk.second.size(), ctx->d_boys64.p, ctx->d_expt64.p, T3.p, ncol};
+      CK(launch_df3c(bc.first.first, bc.first.second, kk.first, a, st));
+    }
+    CK(cudaStreamSynchronize(st));
+  }
+  if (cublasCreate(&df->blas) != CUBLAS_STATUS_SUCCESS) return set_error(ctx, HFG_ERR_CUDA, "cublasCreate");
+  cublasSetStream(df->blas, st);
+  CK(df->B64.alloc((size_t)rank * ncol));
+  {
+    // column-major view: T3c (ncol x naux), Xm (naux x rank) -> Bc (ncol x rank) = B row-major [rank][ncol]
+    const double one = 1.0, zero = 0.0;
+    if (cublasDgemm(df->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)ncol, rank, naux, &one, T3.p, (int)ncol, V.p, naux, &zero,
+                    df->B64.p, (int)ncol) != CUBLAS_STATUS_SUCCESS)
+      return set_error(ctx, HFG_ERR_CUDA, "B = X^T (P|mn) GEMM failed");
+  }
+  T3.release();
+  if (storage == HFG_DF_FP32) {
+    CK(df->B32.alloc((size_t)rank * ncol));
+    CK(launch_convert(1, df->B64.p, df->B32.p, (long long)rank * ncol, st));
+  } else if (storage == HFG_DF_BF16) {
+    CK(df->B16.alloc((size_t)rank * ncol));
+    CK(launch_convert(2, df->B64.p, df->B16.p, (long long)rank * ncol, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  if (storage != HFG_DF_FP64) df->B64.release();
+  *out = df.release();
+#undef CK
+  return HFG_OK;
+}
+
+int hfg_df_destroy(hfg_df* df) {
+  if (!df) return HFG_OK;
+  cudaSetDevice(df->ctx->device);
+  cudaStreamSynchronize(df->ctx->stream);
+  delete df;
+  return HFG_OK;
+}
+
+int hfg_df_sizes(const hfg_df* df, int* naux, int* rank, long long* ncol) {
+  if (!df) return HFG_ERR_INVALID_INPUT;
+  if (naux) *naux = df->naux;
+  if (rank) *rank = df->rank;
+  if (ncol) *ncol = df->ncol;
+  return HFG_OK;
+}
+
+int hfg_df_metric(hfg_df* df, double* M) {
+  if (!df || !M) return HFG_ERR_INVALID_INPUT;
+  cudaSetDevice(df->ctx->device);
+  const size_t len = (size_t)df->naux * df->naux;
+  if (cudaMemcpy(M, df->metric.p, len * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_error(df->ctx, HFG_ERR_CUDA, "copy metric");
+  return HFG_OK;
+}
+
+}  // extern "C"
+
+namespace hfg {
+
+// J and K from occupied coefficients on the device: dC column-major n x nocc
+// (leading dimension n), i.e. the first nocc columns of an SCF C matrix.
+int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK, int mma) {
+  hfg_ctx* ctx = df->ctx;
+  cudaStream_t st = ctx->stream;
+  const int n = df->n, rank = df->rank;
+  const long long ncol = df->ncol, nn = (long long)n * n;
+  int rc = HFG_OK;
+#define CK(call)                         \
+  do {                                   \
+    rc = cuda_check(ctx, (call), #call); \
+    if (rc != HFG_OK) return rc;         \
+  } while (0)
+  if (df->storage == HFG_DF_FP64 && mma != HFG_DF_FP64) mma = HFG_DF_FP64;
+  if (df->storage == HFG_DF_FP32 && mma == HFG_DF_FP64) mma = HFG_DF_FP32;
+  if (df->storage == HFG_DF_BF16) mma = HFG_DF_BF16;
+  if (df->storage == HFG_DF_FP32 && mma == HFG_DF_BF16) mma = HFG_DF_FP32;
+  const double one = 1.0, zero = 0.0, two = 2.0;
+  // P = 2 C C^T
+  CK(df->P.alloc(nn));
+  if (cublasDgemm(df->blas, CUBLAS_OP_N, CUBLAS_OP_T, n, n, nocc, &two, dC, n, dC, n, &zero, df->P.p, n) !=
+      CUBLAS_STATUS_SUCCESS)
+    return set_error(ctx, HFG_ERR_CUDA, "P GEMM");
+  // J: gamma = B p, j = B^T gamma (B row-major [rank][ncol] = column-major ncol x rank)
+  CK(df->pvec.alloc(ncol));
+  CK(df->gam.alloc(rank));
+  CK(df->jcol.alloc(ncol));
+  CK(launch_pack_density(df->P.p, df->colmn.p, ncol, n, df->pvec.p, st));
+  if (df->storage == HFG_DF_FP64) {
+    cublasDgemv(df->blas, CUBLAS_OP_T, (int)ncol, rank, &one, df->B64.p, (int)ncol, df->pvec.p, 1, &zero, df->gam.p, 1);
+    cublasDgemv(df->blas, CUBLAS_OP_N, (int)ncol, rank, &one, df->B64.p, (int)ncol, df->gam.p, 1, &zero, df->jcol.p, 1);
+  } else {
+    // FP32 accumulation of the packed contractions on the stored precision
+    const bool bf = df->storage == HFG_DF_BF16;
+    const void* Bp = bf ? (const void*)df->B16.p : (const void*)df->B32.p;
+    const cudaDataType bt = bf ? CUDA_R_16BF : CUDA_R_32F;
+    CK(df->pvec32.alloc(ncol));
+    CK(df->gam32.alloc(rank));
+    CK(df->jcol32.alloc(ncol));
+    DevBuf<__nv_bfloat16> pv16, g16;
+    CK(launch_convert(1, df->pvec.p, df->pvec32.p, ncol, st));
+    const void* pv = df->pvec32.p;
+    cudaDataType pt = CUDA_R_32F;
+    if (bf) {
+      CK(pv16.alloc(ncol));
+      CK(launch_convert(2, df->pvec.p, pv16.p, ncol, st));
+      pv = pv16.p;
+      pt = CUDA_R_16BF;
+    }
+    rc = gemm_ex(ctx, df->blas, CUBLAS_OP_T, CUBLAS_OP_N, rank, 1, (int)ncol, Bp, bt, (int)ncol, pv, pt, (int)ncol,
+                 0.0f, df->gam32.p, rank, CUBLAS_COMPUTE_32F);
+    if (rc != HFG_OK) return rc;
+    const void* gv = df->gam32.p;
+    cudaDataType gt = CUDA_R_32F;
+    if (bf) {
+      CK(g16.alloc(rank));
+      CK(launch_convert_f32(2, df->gam32.p, g16.p, rank, st));
+      gv = g16.p;
+      gt = CUDA_R_16BF;
+    }
+    rc = gemm_ex(ctx, df->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)ncol, 1, rank, Bp, bt, (int)ncol, gv, gt, rank, 0.0f,
+                 df->jcol32.p, (int)ncol, CUBLAS_COMPUTE_32F);
+    if (rc != HFG_OK) return rc;
+    CK(cudaMemsetAsync(df->jcol.p, 0, ncol * 8, st));
+    CK(launch_accumulate_f32(df->jcol.p, df->jcol32.p, 1.0, ncol, st));
+  }
+  CK(cudaMemsetAsync(dJ, 0, nn * 8, st));
+  CK(launch_unpack_j(df->jcol.p, df->colmn.p, ncol, n, dJ, st));
+
+  // K: chunks of qc auxiliary functions
+  const size_t esz = mma == HFG_DF_FP64 ? 8 : (mma == HFG_DF_FP32 ? 4 : 2);
+  const size_t budget = (size_t)1 << 30;
+  int qc = (int)std::max<size_t>(1, std::min<size_t>((size_t)rank, budget / ((size_t)nn * esz)));
+  CK(df->dense.alloc((size_t)qc * nn * esz));
+  CK(cudaMemsetAsync(dK, 0, nn * 8, st));
+  if (mma == HFG_DF_FP64) {
+    CK(df->T64.alloc((size_t)qc * n * nocc));
+    for (int q0 = 0; q0 < rank; q0 += qc) {
+      const int qn = std::min(qc, rank - q0);
+      CK(cudaMemsetAsync(df->dense.p, 0, (size_t)qn * nn * 8, st));
+      CK(launch_df_unpack(0, df->B64.p, ncol, df->colmn.p, ncol, q0, qn, n, df->dense.p, st));
+      const double* Bd = (const double*)df->dense.p;
+      // T^T (nocc x n*qn) = C^T (nocc x n) * Bd2^T (n x n*qn)
+      cublasDgemm(df->blas, CUBLAS_OP_T, CUBLAS_OP_N, nocc, n * qn, n, &one, dC, n, Bd, n, &zero, df->T64.p, nocc);
+      // K += 2 U U^T, U (row-major n x qn*nocc) = column-major (qn*nocc x n)
+      cublasDgemm(df->blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, qn * nocc, &two, df->T64.p, qn * nocc, df->T64.p,
+                  qn * nocc, &one, dK, n);
+    }
+  } else {
+    const bool bf = mma == HFG_DF_BF16;
+    const cudaDataType it = bf ? CUDA_R_16BF : CUDA_R_32F;
+    const cublasComputeType_t ct = bf ? CUBLAS_COMPUTE_32F : CUBLAS_COMPUTE_32F_FAST_TF32;
+    CK(df->Tf.alloc((size_t)qc * n * nocc));
+    CK(df->Kf.alloc(nn));
+    const void* Cin;
+    if (bf) {
+      CK(df->Cb.alloc((size_t)n * nocc));
+      CK(launch_convert(2, dC, df->Cb.p, (long long)n * nocc, st));
+      Cin = df->Cb.p;
+      CK(df->Tb.alloc((size_t)qc * n * nocc));
+    } else {
+      CK(df->Cf.alloc((size_t)n * nocc));
+      CK(launch_convert(1, dC, df->Cf.p, (long long)n * nocc, st));
+      Cin = df->Cf.p;
+    }
+    const void* Bsrc = df->storage == HFG_DF_BF16 ? (const void*)df->B16.p : (const void*)df->B32.p;
+    const int umode = df->storage == HFG_DF_BF16 ? 2 : 1;
+    for (int q0 = 0; q0 < rank; q0 += qc) {
+      const int qn = std::min(qc, rank - q0);
+      CK(cudaMemsetAsync(df->dense.p, 0, (size_t)qn * nn * esz, st));
+      CK(launch_df_unpack(umode, Bsrc, ncol, df->colmn.p, ncol, q0, qn, n, df->dense.p, st));
+      rc = gemm_ex(ctx, df->blas, CUBLAS_OP_T, CUBLAS_OP_N, nocc, n * qn, n, Cin, it, n, df->dense.p, it, n, 0.0f,
+                   df->Tf.p, nocc, ct);
+      if (rc != HFG_OK) return rc;
+      const void* U = df->Tf.p;
+      if (bf) {
+        // T (FP32 accumulated) back to BF16 for the second product
+        CK(launch_convert_f32(2, df->Tf.p, df->Tb.p, (long long)qn * n * nocc, st));
+        U = df->Tb.p;
+      }
+      rc = gemm_ex(ctx, df->blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, qn * nocc, U, it, qn * nocc, U, it, qn * nocc, 0.0f,
+                   df->Kf.p, n, ct);
+      if (rc != HFG_OK) return rc;
+      CK(launch_accumulate_f32(dK, df->Kf.p, 2.0, nn, st));
+    }
+  }
+#undef CK
+  return HFG_OK;
+}
+
+}  // namespace hfg
+
+extern "C" int hfg_df_jk(hfg_df* df, const double* C_occ, int nocc, double* J, double* K, int mma) {
+  if (!df || !C_occ || !J || !K || nocc <= 0) return HFG_ERR_INVALID_INPUT;
+  hfg_ctx* ctx = df->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  const long long nn = (long long)df->n * df->n;
+  int rc = cuda_check(ctx, df->Cd.alloc((size_t)df->n * nocc), "alloc");
+  if (rc == HFG_OK) rc = cuda_check(ctx, df->J.alloc(nn), "alloc");
+  if (rc == HFG_OK) rc = cuda_check(ctx, df->K.alloc(nn), "alloc");
+  if (rc != HFG_OK) return rc;
+  // row-major n x nocc -> column-major (leading dimension n)
+  std::vector<double> ct((size_t)df->n * nocc);
+  for (int i = 0; i < df->n; ++i)
+    for (int k = 0; k < nocc; ++k) ct[(size_t)k * df->n + i] = C_occ[(size_t)i * nocc + k];
+  cudaMemcpyAsync(df->Cd.p, ct.data(), ct.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+  rc = df_jk_device(df, df->Cd.p, nocc, df->J.p, df->K.p, mma);
+  if (rc != HFG_OK) return rc;
+  cudaMemcpyAsync(J, df->J.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(K, df->K.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "df_jk sync");
+}

@@ -200,6 +200,24 @@ def gen_class(la, lb, lc, ld):
     return "\n".join(s), v.count, len(hl)
 
 
+def class_list(lmax):
+    """Four-centre classes with l <= lmax, plus the density-fitting classes
+    (la lb|lc 0): orbital pairs (la, lb <= 2) or an auxiliary function with a
+    unit partner (la <= 4, lb = 0) against an auxiliary function (lc <= 4)."""
+    out = []
+    for la in range(lmax + 1):
+        for lb in range(la + 1):
+            for lc in range(lmax + 1):
+                for ld in range(lc + 1):
+                    out.append((la, lb, lc, ld))
+    bras = [(la, lb) for la in range(3) for lb in range(la + 1)] + [(3, 0), (4, 0)]
+    for la, lb in bras:
+        for lc in range(5):
+            if (la, lb, lc, 0) not in out:
+                out.append((la, lb, lc, 0))
+    return out
+
+
 def main():
     lmax = int(sys.argv[1]) if len(sys.argv) > 1 else 2
     here = os.path.dirname(os.path.abspath(__file__))
@@ -209,13 +227,10 @@ def main():
              "template <int LA, int LB, int LC, int LD> struct EriClass;",
              "#define T(n) static_cast<T>(n)"]
     stats = []
-    for la in range(lmax + 1):
-        for lb in range(la + 1):
-            for lc in range(lmax + 1):
-                for ld in range(lc + 1):
-                    code, nv, nh = gen_class(la, lb, lc, ld)
-                    parts.append(code)
-                    stats.append((la, lb, lc, ld, nv, nh))
+    for la, lb, lc, ld in class_list(lmax):
+        code, nv, nh = gen_class(la, lb, lc, ld)
+        parts.append(code)
+        stats.append((la, lb, lc, ld, nv, nh))
     parts.append("#undef T")
     parts.append("}  // namespace hfg")
     with open(os.path.join(here, "eri_gen.cuh"), "w") as f:

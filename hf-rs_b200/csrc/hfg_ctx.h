@@ -96,10 +96,16 @@ struct hfg_ctx {
   ~hfg_ctx();
 };
 
+struct hfg_df;
+
 namespace hfg {
+// Implemented in df.cu: DF J/K from column-major occupied coefficients.
+int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK, int mma);
 // Implemented in ctx.cu, used by scf.cu.
 int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs,
                      double* dJ, double* dK);
 int set_error(hfg_ctx* ctx, int code, const std::string& msg);
+int build_shell_list(hfg_ctx* ctx, const hfg_basis* b, int lmax);
+void make_pair(const hfg_ctx* ctx, int a, int b, PairInfo& pi, std::vector<PrimPair>& pp, int owner);
 int cuda_check(hfg_ctx* ctx, cudaError_t e, const char* what);
 }  // namespace hfg

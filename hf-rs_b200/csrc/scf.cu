@@ -221,60 +221,23 @@ struct Scf {
 }  // namespace
 }  // namespace hfg
 
-using namespace hfg;
-
-extern "C" {
-
-void hfg_scf_opts_default(hfg_scf_opts* o) {
-  if (!o) return;
-  *o = hfg_scf_opts{};
-  o->multiplicity = 1;
-  o->max_iter = 100;
-  o->energy_tol = 1e-10;
-  o->residual_tol = std::max(std::sqrt(1e-10) * 1e-2, 1e-11);
-  o->density_tol = std::min(std::max(std::sqrt(1e-10) * 0.1, 1e-12), 1e-10);
-  hfg_jk_opts_default(&o->jk);
-  o->refine_iters = 2;
-  o->diis_size = 8;
-}
-
-int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_out, double* F_out, double* C_out,
-            double* eps_out) {
-  if (!ctx || !o || !res) return HFG_ERR_INVALID_INPUT;
-  auto t_start = std::chrono::steady_clock::now();
-  std::lock_guard<std::mutex> lk(ctx->mu);
-  cudaSetDevice(ctx->device);
-  *res = hfg_scf_result{};
+namespace hfg {
+namespace {
+// One-electron integrals, H = T + V, and the orthogonaliser X (n x m) of the
+// Cartesian or real spherical AO space with cutoff 1e-8.
+int scf_setup(hfg_ctx* ctx, const hfg_scf_opts* o, Scf& s, int& m_out) {
   const int n = ctx->n;
-  if (o->natom <= 0 || !o->positions || !o->charges)
-    return set_error(ctx, HFG_ERR_INVALID_INPUT, "SCF requires nuclei");
-  if (o->max_iter <= 0 || !(o->energy_tol > 0) || !(o->residual_tol > 0) || !(o->density_tol > 0))
-    return set_error(ctx, HFG_ERR_INVALID_INPUT, "SCF requires a positive tolerance and iteration limit");
-  for (int a = 0; a < 3 * o->natom; ++a)
-    if (!std::isfinite(o->positions[a])) return set_error(ctx, HFG_ERR_INVALID_INPUT, "non-finite geometry");
-  double zsum = 0.0;
-  for (int a = 0; a < o->natom; ++a) zsum += o->charges[a];
-  const int nel = (int)std::lround(zsum) - o->charge;
-  if (nel <= 0) return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid electron count");
-  const bool uhf = o->uhf != 0;
-  const int two_s = o->multiplicity - 1;
-  if (o->multiplicity < 1 || two_s > nel || ((nel + two_s) & 1))
-    return set_error(ctx, HFG_ERR_INVALID_INPUT, "incompatible electron count and multiplicity");
-  if (!uhf && (nel & 1)) return set_error(ctx, HFG_ERR_INVALID_INPUT, "RHF requires an even number of electrons");
-  const int na = uhf ? (nel + two_s) / 2 : nel / 2, nb = uhf ? (nel - two_s) / 2 : nel / 2;
-  const int nspin = uhf ? 2 : 1;
-  // nuclear repulsion (src/scf.rs:207-218)
-  double e_nuc = 0.0;
-  for (int i = 0; i < o->natom; ++i)
-    for (int j = i + 1; j < o->natom; ++j) {
-      const double dx = o->positions[3 * i] - o->positions[3 * j], dy = o->positions[3 * i + 1] - o->positions[3 * j + 1],
-                   dz = o->positions[3 * i + 2] - o->positions[3 * j + 2];
-      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
-      if (d < 1e-8) return set_error(ctx, HFG_ERR_INVALID_INPUT, "coincident nuclei");
-      e_nuc += o->charges[i] * o->charges[j] / d;
-    }
-
-  Scf s;
+  int rc = HFG_OK;
+#define CK(call)                         \
+  do {                                   \
+    rc = cuda_check(ctx, (call), #call); \
+    if (rc != HFG_OK) return rc;         \
+  } while (0)
+#define RK(call)                 \
+  do {                           \
+    rc = (call);                 \
+    if (rc != HFG_OK) return rc; \
+  } while (0)
   s.ctx = ctx;
   s.n = n;
   if (cublasCreate(&s.blas) != CUBLAS_STATUS_SUCCESS) return set_error(ctx, HFG_ERR_CUDA, "cublasCreate");
@@ -282,17 +245,6 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   cublasSetStream(s.blas, ctx->stream);
   cusolverDnSetStream(s.solver, ctx->stream);
   const long long nn = (long long)n * n;
-  int rc = HFG_OK;
-#define CK(call)                                    \
-  do {                                              \
-    rc = cuda_check(ctx, (call), #call);            \
-    if (rc != HFG_OK) return rc;                    \
-  } while (0)
-#define RK(call)             \
-  do {                       \
-    rc = (call);             \
-    if (rc != HFG_OK) return rc; \
-  } while (0)
   CK(s.S.alloc(nn));
   CK(s.H.alloc(nn));
   CK(s.T.alloc(nn));
@@ -361,7 +313,6 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   while (first < nsph && w[first] < 1e-8) ++first;
   const int m = nsph - first;
   if (m <= 0) return set_error(ctx, HFG_ERR_INTEGRAL, "overlap has zero retained rank");
-  if (na > m || nb > m) return set_error(ctx, HFG_ERR_INVALID_INPUT, "more occupied orbitals than retained rank");
   s.m = m;
   // U_keep / sqrt(w), then X = T U_keep diag(w^-1/2)  (n x m)
   phase_kernel<<<nsph, 256, 0, ctx->stream>>>(s.tmp2.p, nsph, nsph);
@@ -370,6 +321,86 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   CK(s.X.alloc((size_t)n * m));
   RK(s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, m, nsph, 1.0, dT2.p, n, s.tmp2.p + (size_t)first * nsph, nsph, 0.0, s.X.p, n));
 
+  m_out = m;
+  return HFG_OK;
+#undef CK
+#undef RK
+}
+}  // namespace
+}  // namespace hfg
+
+using namespace hfg;
+
+extern "C" {
+
+void hfg_scf_opts_default(hfg_scf_opts* o) {
+  if (!o) return;
+  *o = hfg_scf_opts{};
+  o->multiplicity = 1;
+  o->max_iter = 100;
+  o->energy_tol = 1e-10;
+  o->residual_tol = std::max(std::sqrt(1e-10) * 1e-2, 1e-11);
+  o->density_tol = std::min(std::max(std::sqrt(1e-10) * 0.1, 1e-12), 1e-10);
+  hfg_jk_opts_default(&o->jk);
+  o->refine_iters = 2;
+  o->diis_size = 8;
+}
+
+int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_out, double* F_out, double* C_out,
+            double* eps_out) {
+  if (!ctx || !o || !res) return HFG_ERR_INVALID_INPUT;
+  auto t_start = std::chrono::steady_clock::now();
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  *res = hfg_scf_result{};
+  const int n = ctx->n;
+  if (o->natom <= 0 || !o->positions || !o->charges)
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "SCF requires nuclei");
+  if (o->max_iter <= 0 || !(o->energy_tol > 0) || !(o->residual_tol > 0) || !(o->density_tol > 0))
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "SCF requires a positive tolerance and iteration limit");
+  for (int a = 0; a < 3 * o->natom; ++a)
+    if (!std::isfinite(o->positions[a])) return set_error(ctx, HFG_ERR_INVALID_INPUT, "non-finite geometry");
+  double zsum = 0.0;
+  for (int a = 0; a < o->natom; ++a) zsum += o->charges[a];
+  const int nel = (int)std::lround(zsum) - o->charge;
+  if (nel <= 0) return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid electron count");
+  const bool uhf = o->uhf != 0;
+  const int two_s = o->multiplicity - 1;
+  if (o->multiplicity < 1 || two_s > nel || ((nel + two_s) & 1))
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "incompatible electron count and multiplicity");
+  if (!uhf && (nel & 1)) return set_error(ctx, HFG_ERR_INVALID_INPUT, "RHF requires an even number of electrons");
+  const int na = uhf ? (nel + two_s) / 2 : nel / 2, nb = uhf ? (nel - two_s) / 2 : nel / 2;
+  const int nspin = uhf ? 2 : 1;
+  // nuclear repulsion (src/scf.rs:207-218)
+  double e_nuc = 0.0;
+  for (int i = 0; i < o->natom; ++i)
+    for (int j = i + 1; j < o->natom; ++j) {
+      const double dx = o->positions[3 * i] - o->positions[3 * j], dy = o->positions[3 * i + 1] - o->positions[3 * j + 1],
+                   dz = o->positions[3 * i + 2] - o->positions[3 * j + 2];
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      if (d < 1e-8) return set_error(ctx, HFG_ERR_INVALID_INPUT, "coincident nuclei");
+      e_nuc += o->charges[i] * o->charges[j] / d;
+    }
+
+  Scf s;
+  int m = 0;
+  {
+    const int rcs = scf_setup(ctx, o, s, m);
+    if (rcs != HFG_OK) return rcs;
+  }
+  if (na > m || nb > m) return set_error(ctx, HFG_ERR_INVALID_INPUT, "more occupied orbitals than retained rank");
+  const long long nn = (long long)n * n;
+  int rc = HFG_OK;
+#define CK(call)                                    \
+  do {                                              \
+    rc = cuda_check(ctx, (call), #call);            \
+    if (rc != HFG_OK) return rc;                    \
+  } while (0)
+#define RK(call)             \
+  do {                       \
+    rc = (call);             \
+    if (rc != HFG_OK) return rc; \
+  } while (0)
   // state
   const int hist = std::max(2, o->diis_size);
   DevBuf<double> P, Pprev, F, J, K, E, C, Fh, Eh, Fp;
@@ -612,3 +643,170 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
 }
 
 }  // extern "C"
+
+extern "C" int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts* o, hfg_scf_result* res, double* P_out,
+                          double* F_out, double* J_out, double* K_out) {
+  // run_factorized_rhf (src/hf_variants/ri_df_hf.rs:160-263): core guess,
+  // CDIIS from the second iteration, convergence on |dE|, the residual and
+  // max |P_next - P| of the density from the un-extrapolated Fock matrix.
+  if (!ctx || !df || !o || !res) return HFG_ERR_INVALID_INPUT;
+  auto t_start = std::chrono::steady_clock::now();
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  *res = hfg_scf_result{};
+  const int n = ctx->n;
+  double zsum = 0.0;
+  for (int a = 0; a < o->natom; ++a) zsum += o->charges[a];
+  const double electrons = zsum - o->charge;
+  if (!(electrons > 0) || std::fabs(electrons - std::round(electrons)) > 1e-8 || ((long)std::lround(electrons) & 1))
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "factorized RHF requires a positive even electron count");
+  const int no = (int)std::lround(electrons) / 2;
+  double e_nuc = 0.0;
+  for (int i = 0; i < o->natom; ++i)
+    for (int j = i + 1; j < o->natom; ++j) {
+      const double dx = o->positions[3 * i] - o->positions[3 * j], dy = o->positions[3 * i + 1] - o->positions[3 * j + 1],
+                   dz = o->positions[3 * i + 2] - o->positions[3 * j + 2];
+      e_nuc += o->charges[i] * o->charges[j] / std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+  Scf s;
+  int m = 0;
+  {
+    const int rcs = scf_setup(ctx, o, s, m);
+    if (rcs != HFG_OK) return rcs;
+  }
+  if (no > m) return set_error(ctx, HFG_ERR_INVALID_INPUT, "factorized RHF occupied count exceeds overlap rank");
+  const long long nn = (long long)n * n;
+  int rc = HFG_OK;
+#define CK(call)                         \
+  do {                                   \
+    rc = cuda_check(ctx, (call), #call); \
+    if (rc != HFG_OK) return rc;         \
+  } while (0)
+#define RK(call)                 \
+  do {                           \
+    rc = (call);                 \
+    if (rc != HFG_OK) return rc; \
+  } while (0)
+  const int hist = std::max(2, o->diis_size);
+  DevBuf<double> P, Pn, F, J, K, E, C, Cn, Fh, Eh, Fp, Fx;
+  const long long elen = (long long)m * m;
+  const long long elen_eff = m < n ? elen : nn;
+  CK(P.alloc(nn));
+  CK(Pn.alloc(nn));
+  CK(F.alloc(nn));
+  CK(Fx.alloc(nn));
+  CK(J.alloc(nn));
+  CK(K.alloc(nn));
+  CK(E.alloc(std::max(nn, elen)));
+  CK(C.alloc((long long)n * m));
+  CK(Cn.alloc((long long)n * m));
+  CK(Fh.alloc((long long)hist * nn));
+  CK(Eh.alloc((long long)hist * elen));
+  CK(Fp.alloc(std::max(nn, elen)));
+  CK(s.evals.alloc(std::max(n, m)));
+  auto diag = [&](const double* Fm, double* Cm, double* Pm) -> int {
+    RK(s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, m, n, 1.0, Fm, n, s.X.p, n, 0.0, s.tmp1.p, n));
+    RK(s.gemm(CUBLAS_OP_T, CUBLAS_OP_N, m, m, n, 1.0, s.X.p, n, s.tmp1.p, n, 0.0, Fp.p, m));
+    RK(s.eigh(Fp.p, s.evals.p, m));
+    phase_kernel<<<m, 256, 0, ctx->stream>>>(Fp.p, m, m);
+    RK(s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, 1.0, s.X.p, n, Fp.p, m, 0.0, Cm, n));
+    RK(s.gemm(CUBLAS_OP_N, CUBLAS_OP_T, n, n, no, 2.0, Cm, n, Cm, n, 0.0, Pm, n));
+    return HFG_OK;
+  };
+  auto fock = [&](const double* Cm) -> int {
+    RK(df_jk_device(df, Cm, no, J.p, K.p, mma));
+    CK(cudaMemcpyAsync(F.p, s.H.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(F.p, J.p, 1.0, 1.0, nn);
+    axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(F.p, K.p, -0.5, 1.0, nn);
+    return HFG_OK;
+  };
+  auto energy = [&](const double* Pm) { return 0.5 * (s.dot(Pm, s.H.p, nn) + s.dot(Pm, F.p, nn)) + e_nuc; };
+  RK(diag(s.H.p, C.p, P.p));
+  double last = INFINITY;
+  bool converged = false;
+  int it = 0, count = 0;
+  std::vector<int> slot;
+  std::vector<double> Bm;
+  for (it = 1; it <= o->max_iter; ++it) {
+    RK(fock(C.p));
+    const double e = energy(P.p);
+    // residual X^T (FPS - SPF) X
+    RK(s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, F.p, n, P.p, n, 0.0, s.tmp1.p, n));
+    RK(s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, s.tmp1.p, n, s.S.p, n, 0.0, s.T.p, n));
+    antisym_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(s.T.p, s.V.p, n);
+    RK(s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, m, n, 1.0, s.V.p, n, s.X.p, n, 0.0, s.tmp1.p, n));
+    RK(s.gemm(CUBLAS_OP_T, CUBLAS_OP_N, m, m, n, 1.0, s.X.p, n, s.tmp1.p, n, 0.0, E.p, m));
+    const double resid = s.maxabs(E.p, elen);
+    RK(diag(F.p, Cn.p, Pn.p));
+    CK(cudaMemcpyAsync(s.tmp1.p, Pn.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(s.tmp1.p, P.p, -1.0, 1.0, nn);
+    const double dch = s.maxabs(s.tmp1.p, nn);
+    if (!std::isfinite(e) || !std::isfinite(resid)) return set_error(ctx, HFG_ERR_SCF, "DF-HF energy/residual became nonfinite");
+    if (o->verbose) fprintf(stderr, "hfg df-scf %3d  E = %.12f  |e| = %.3e  dP = %.3e\n", it, e, resid, dch);
+    if (std::fabs(e - last) <= o->energy_tol && resid <= o->residual_tol && dch <= o->density_tol) {
+      RK(fock(Cn.p));
+      const double ef = energy(Pn.p);
+      res->energy = ef;
+      res->electronic = ef - e_nuc;
+      res->nuclear = e_nuc;
+      res->energy_before_refinement = ef;
+      converged = true;
+      break;
+    }
+    last = e;
+    int sl;
+    if (count < hist) {
+      sl = count++;
+      slot.push_back(sl);
+    } else {
+      sl = slot.front();
+      slot.erase(slot.begin());
+      slot.push_back(sl);
+    }
+    CK(cudaMemcpyAsync(Fh.p + (long long)sl * nn, F.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(Eh.p + (long long)sl * elen, E.p, elen * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    const int k = (int)slot.size();
+    std::vector<double> Bn((size_t)k * k);
+    {
+      const int kprev = (int)std::sqrt((double)Bm.size());
+      for (int i = 0; i < k - 1; ++i)
+        for (int j = 0; j < k - 1; ++j) Bn[(size_t)i * k + j] = Bm[(size_t)(kprev - (k - 1) + i) * kprev + kprev - (k - 1) + j];
+      for (int i = 0; i < k; ++i) {
+        const double d = s.dot(Eh.p + (long long)slot[i] * elen, Eh.p + (long long)sl * elen, elen);
+        Bn[(size_t)i * k + (k - 1)] = Bn[(size_t)(k - 1) * k + i] = d;
+      }
+    }
+    Bm = Bn;
+    const double* Fuse = F.p;
+    if (it >= 2 && k >= 2) {
+      const int dim = k + 1;
+      std::vector<double> A((size_t)dim * dim, 0.0), x(dim, 0.0);
+      for (int i = 0; i < k; ++i) {
+        for (int j = 0; j < k; ++j) A[(size_t)i * dim + j] = Bm[(size_t)i * k + j];
+        A[(size_t)i * dim + k] = A[(size_t)k * dim + i] = -1.0;
+      }
+      x[k] = -1.0;
+      if (solve_small(A, x, dim)) {
+        CK(cudaMemsetAsync(Fx.p, 0, nn * 8, ctx->stream));
+        for (int i = 0; i < k; ++i)
+          axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(Fx.p, Fh.p + (long long)slot[i] * nn, x[i], 1.0, nn);
+        Fuse = Fx.p;
+      }
+    }
+    RK(diag(Fuse, C.p, P.p));
+  }
+  (void)elen_eff;
+  if (it > o->max_iter) it = o->max_iter;
+  res->iterations = it;
+  res->converged = converged ? 1 : 0;
+  res->n_mo = m;
+  if (P_out) CK(cudaMemcpyAsync(P_out, Pn.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (F_out) CK(cudaMemcpyAsync(F_out, F.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (J_out) CK(cudaMemcpyAsync(J_out, J.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (K_out) CK(cudaMemcpyAsync(K_out, K.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  res->time_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+#undef CK
+#undef RK
+  return converged ? HFG_OK : set_error(ctx, HFG_ERR_SCF, "factorized RHF did not converge");
+}

@@ -117,6 +117,12 @@ def load_library():
     L.hfg_jk_last_stats.argtypes = [VP, P(JKStats)]
     L.hfg_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, DP]
     L.hfg_scf_opts_default.argtypes = [P(SCFOptions)]
+    L.hfg_df_build.argtypes = [VP, P(HfgBasis), ctypes.c_double, ctypes.c_double, ctypes.c_int, P(VP)]
+    L.hfg_df_destroy.argtypes = [VP]
+    L.hfg_df_sizes.argtypes = [VP, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_longlong)]
+    L.hfg_df_metric.argtypes = [VP, DP]
+    L.hfg_df_jk.argtypes = [VP, DP, ctypes.c_int, DP, DP, ctypes.c_int]
+    L.hfg_scf_df.argtypes = [VP, VP, ctypes.c_int, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     L.hfg_scf.argtypes = [VP, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     _lib = L
     return L
@@ -259,7 +265,90 @@ class Context:
                     "eps": None if eps is None else eps[:, :m], "status": rc})
         return out
 
+    def _scf_opts(self, charge, multiplicity, uhf, spherical, tol, max_iter, jk, refine_iters, verbose, keep):
+        b = self.basis
+        o = SCFOptions()
+        self.lib.hfg_scf_opts_default(ctypes.byref(o))
+        pos = np.ascontiguousarray(b.positions())
+        chg = np.ascontiguousarray(b.nuclear_charges())
+        keep.extend([pos, chg])
+        o.natom = len(chg)
+        o.positions = _dp(pos)
+        o.charges = _dp(chg)
+        o.charge, o.multiplicity, o.uhf, o.spherical = charge, multiplicity, int(uhf), int(spherical)
+        o.max_iter = max_iter
+        if isinstance(tol, tuple):
+            o.energy_tol, o.residual_tol, o.density_tol = tol
+        else:
+            o.energy_tol, o.residual_tol, o.density_tol = convergence_from_tol(tol)
+        o.jk = jk or JKOptions.make()
+        o.refine_iters = refine_iters
+        o.verbose = int(verbose)
+        return o
+
+    def scf_df(self, df, mma=0, charge=0, spherical=False, tol=(1e-12, 1e-10, 1e-10), max_iter=100, verbose=False):
+        """DF-RHF (hfg_scf_df) with a DFTensor built on this context."""
+        keep = []
+        o = self._scf_opts(charge, 1, False, spherical, tol, max_iter, None, 0, verbose, keep)
+        n = self.n
+        P, F, J, K = (np.zeros((n, n)) for _ in range(4))
+        r = SCFResult()
+        rc = self.lib.hfg_scf_df(self.h, df.h, mma, ctypes.byref(o), ctypes.byref(r), _dp(P), _dp(F), _dp(J), _dp(K))
+        if rc not in (0, 3):
+            self._check(rc)
+        out = r.as_dict()
+        out.update({"P": P, "F": F, "J": J, "K": K, "status": rc})
+        return out
+
     def last_stats(self):
         s = JKStats()
         self._check(self.lib.hfg_jk_last_stats(self.h, ctypes.byref(s)))
         return s.as_dict()
+
+
+HFG_DF_FP64, HFG_DF_FP32, HFG_DF_BF16 = 0, 1, 2
+
+
+class DFTensor:
+    """hfg_df: the DF factor B = X^T (P|mn) of an auxiliary basis on a context."""
+
+    def __init__(self, ctx, aux, metric_cutoff=1e-10, pair_threshold=0.0, storage=HFG_DF_FP64):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.aux = aux
+        self._b = HfgBasis(aux.n, _dp(aux.center), _ip(aux.lxyz), _ip(aux.atom), _ip(aux.prim_off), _dp(aux.exps),
+                           _dp(aux.coefs))
+        h = VP()
+        rc = self.lib.hfg_df_build(ctx.h, ctypes.byref(self._b), metric_cutoff, pair_threshold, storage,
+                                   ctypes.byref(h))
+        ctx._check(rc)
+        self.h = h
+
+    def sizes(self):
+        a, r, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        self.ctx._check(self.lib.hfg_df_sizes(self.h, ctypes.byref(a), ctypes.byref(r), ctypes.byref(c)))
+        return a.value, r.value, c.value
+
+    def metric(self):
+        naux = self.sizes()[0]
+        M = np.zeros((naux, naux))
+        self.ctx._check(self.lib.hfg_df_metric(self.h, _dp(M)))
+        return M
+
+    def jk(self, C_occ, mma=HFG_DF_FP64):
+        n = self.ctx.n
+        C = np.ascontiguousarray(C_occ, dtype=np.float64)
+        J, K = np.zeros((n, n)), np.zeros((n, n))
+        self.ctx._check(self.lib.hfg_df_jk(self.h, _dp(C), C.shape[1], _dp(J), _dp(K), mma))
+        return J, K
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.hfg_df_destroy(self.h)
+            self.h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

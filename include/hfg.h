@@ -143,6 +143,32 @@ typedef struct {
 } hfg_jk_stats;
 int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* stats);
 
+/* Density fitting (src/df.rs, src/hf_variants/ri_df_hf.rs). */
+typedef enum { HFG_DF_FP64 = 0, HFG_DF_FP32 = 1, HFG_DF_BF16 = 2 } hfg_df_precision;
+typedef struct hfg_df hfg_df;
+
+/*
+ * Stands in for DfTensor::build (src/df.rs:89-127, Cartesian auxiliary
+ * space): the Coulomb metric (P|Q), its canonical orthogonaliser with
+ * `metric_cutoff` (src/df.rs:16-28), the three-centre integrals (P|mn) and
+ * B = X^T (P|mn), all on the device.  B keeps the unique AO pairs of the
+ * shell pairs whose Schwarz bound exceeds `pair_threshold` (0 keeps all, as
+ * hf-rs) and is stored in `storage` precision (hfg_df_precision).
+ */
+int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, double pair_threshold, int storage,
+                 hfg_df** out);
+int hfg_df_destroy(hfg_df* df);
+int hfg_df_sizes(const hfg_df* df, int* naux, int* rank, long long* ncol);
+/* The metric (P|Q) as built (naux x naux, row-major). */
+int hfg_df_metric(hfg_df* df, double* M);
+/*
+ * Stands in for DfTensor::coulomb_exchange_rhf (src/df.rs:133-174): J and K
+ * of the density 2 C_occ C_occ^T, C_occ row-major n x nocc (host).  `mma`
+ * selects the K GEMMs: FP64, TF32 (FP32 storage) or BF16 tensor cores with
+ * FP32 accumulation, summed into FP64.
+ */
+int hfg_df_jk(hfg_df* df, const double* C_occ, int nocc, double* J, double* K, int mma);
+
 /* Options of hfg_scf: nuclei, electrons, AO space and convergence controls of
    run_scf_in_space_with_convergence / run_uhf_in_space_with_convergence
    (src/scf.rs:410, :691; RhfConvergence src/scf.rs:400-407). */
@@ -188,6 +214,17 @@ void hfg_scf_opts_default(hfg_scf_opts* opts);
  */
 int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* opts, hfg_scf_result* result, double* P, double* F, double* C,
             double* eps);
+
+/*
+ * Stands in for run_df_hf_with_aux / run_factorized_rhf
+ * (src/hf_variants/ri_df_hf.rs:122-263): DF-RHF with the DF tensor `df`
+ * built on this context, K GEMMs in `mma` precision.  Uses the nuclei,
+ * charge, AO space, iteration limit, tolerances and DIIS size of `opts`.
+ * Optional outputs (row-major n x n, NULL to skip): P, F, J, K at
+ * convergence.
+ */
+int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts* opts, hfg_scf_result* result, double* P,
+               double* F, double* J, double* K);
 
 /* Measured FMA-pipe peak of the device in TFLOP/s (FP64 when fp32 == 0):
    independent FMA chains in registers on every SM.  The roofline
