@@ -19,6 +19,8 @@ using namespace hfg;
 
 namespace hfg {
 
+thread_local cudaStream_t tl_alloc_stream = nullptr;
+
 int set_error(hfg_ctx* ctx, int code, const std::string& msg) {
   if (ctx) ctx->err = msg;
   return code;
@@ -408,12 +410,14 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     return std::make_tuple(x.la + x.lb + x.lc + x.ld, x.fp32) > std::make_tuple(y.la + y.lb + y.lc + y.ld, y.fp32);
   });
   for (auto& L : plan->launches) {
-    HFG_CUDA(ctx, cudaMalloc(&L.d_entries, L.entries.size() * sizeof(JKEntry)));
-    HFG_CUDA(ctx, cudaMalloc(&L.d_prefix, L.prefix.size() * sizeof(long long)));
-    HFG_CUDA(ctx, cudaMemcpy(L.d_entries, L.entries.data(), L.entries.size() * sizeof(JKEntry),
-                             cudaMemcpyHostToDevice));
-    HFG_CUDA(ctx, cudaMemcpy(L.d_prefix, L.prefix.data(), L.prefix.size() * sizeof(long long),
-                             cudaMemcpyHostToDevice));
+    L.st = ctx->stream;
+    HFG_CUDA(ctx, cudaMallocAsync((void**)&L.d_entries, L.entries.size() * sizeof(JKEntry), ctx->stream));
+    HFG_CUDA(ctx, cudaMallocAsync((void**)&L.d_prefix, L.prefix.size() * sizeof(long long), ctx->stream));
+    HFG_CUDA(ctx, cudaMemcpyAsync(L.d_entries, L.entries.data(), L.entries.size() * sizeof(JKEntry),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    HFG_CUDA(ctx, cudaMemcpyAsync(L.d_prefix, L.prefix.data(), L.prefix.size() * sizeof(long long),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     // the host copies are no longer needed beyond the counts
     const size_t ne = L.entries.size();
     const long long nw = L.prefix.back();
@@ -554,8 +558,8 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
 hfg_ctx::~hfg_ctx() {
   for (auto& kv : plans)
     for (auto& L : kv.second->launches) {
-      if (L.d_entries) cudaFree(L.d_entries);
-      if (L.d_prefix) cudaFree(L.d_prefix);
+      if (L.d_entries) cudaFreeAsync(L.d_entries, L.st);
+      if (L.d_prefix) cudaFreeAsync(L.d_prefix, L.st);
     }
   d_pairs.release();
   d_prims.release();
@@ -600,6 +604,19 @@ int hfg_ctx_create(const hfg_basis* basis, int device, void* stream, hfg_ctx** o
       ctx->own_stream = true;
     }
   }
+  if (rc == HFG_OK) {
+    // keep freed stream-ordered memory in the pool for reuse
+    static std::once_flag pool_once[64];
+    if (device >= 0 && device < 64)
+      std::call_once(pool_once[device], [device] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+          unsigned long long thr = ~0ull;
+          cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+      });
+  }
+  AllocScope alloc_scope(rc == HFG_OK ? ctx->stream : nullptr);
   if (rc == HFG_OK) rc = build_shell_list(ctx.get(), basis, kLMax);
   if (rc == HFG_OK) {
     const auto& t = boys_table_host();
@@ -639,6 +656,7 @@ int hfg_ctx_create(const hfg_basis* basis, int device, void* stream, hfg_ctx** o
 int hfg_ctx_destroy(hfg_ctx* ctx) {
   if (!ctx) return HFG_OK;
   cudaSetDevice(ctx->device);
+  AllocScope alloc_scope(ctx->stream);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   delete ctx;
   return HFG_OK;
@@ -663,6 +681,7 @@ int hfg_schwarz(hfg_ctx* ctx, double* bounds, long n) {
 int hfg_shell_quartet(hfg_ctx* ctx, int a, int b, int c, int d, double* out) {
   if (!ctx || !out) return HFG_ERR_INVALID_INPUT;
   std::lock_guard<std::mutex> lk(ctx->mu);
+  AllocScope alloc_scope(ctx->stream);
   const int ns = (int)ctx->shells.size();
   for (int s : {a, b, c, d})
     if (s < 0 || s >= ns) return set_error(ctx, HFG_ERR_INVALID_INPUT, "shell index out of range");
@@ -710,6 +729,7 @@ int hfg_jk_device(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double
                   double* dK) {
   if (!ctx || !dPt || !dPs || !dJ || !dK) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  AllocScope alloc_scope(ctx->stream);
   cudaSetDevice(ctx->device);
   return jk_device_locked(ctx, opts, nspin, dPt, dPs, dJ, dK);
 }
@@ -719,6 +739,7 @@ int hfg_jk(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* Pt, c
   if (!ctx || !Pt || !Ps || !J || !K) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
   if (nspin < 1 || nspin > 2) return set_error(ctx, HFG_ERR_INVALID_INPUT, "nspin must be 1 or 2");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  AllocScope alloc_scope(ctx->stream);
   cudaSetDevice(ctx->device);
   const size_t nn = (size_t)ctx->n * ctx->n;
   HFG_CUDA(ctx, ctx->d_D.alloc(nn));
@@ -741,6 +762,7 @@ static int fock_common(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, c
                        double* Fa, double* Fb, int uhf) {
   if (!ctx || !H || !Pa || !Fa || (uhf && (!Pb || !Fb))) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  AllocScope alloc_scope(ctx->stream);
   cudaSetDevice(ctx->device);
   const size_t nn = (size_t)ctx->n * ctx->n;
   HFG_CUDA(ctx, ctx->d_D.alloc(nn));

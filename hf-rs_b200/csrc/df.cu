@@ -72,6 +72,7 @@ int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, doubl
   if (storage < HFG_DF_FP64 || storage > HFG_DF_BF16) return set_error(ctx, HFG_ERR_INVALID_INPUT, "storage");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
+  AllocScope alloc_scope(ctx->stream);
   auto df = std::make_unique<hfg_df>();
   df->ctx = ctx;
   df->n = ctx->n;
@@ -245,6 +246,7 @@ int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, doubl
 int hfg_df_destroy(hfg_df* df) {
   if (!df) return HFG_OK;
   cudaSetDevice(df->ctx->device);
+  AllocScope alloc_scope(df->ctx->stream);
   cudaStreamSynchronize(df->ctx->stream);
   delete df;
   return HFG_OK;
@@ -408,6 +410,7 @@ extern "C" int hfg_df_jk(hfg_df* df, const double* C_occ, int nocc, double* J, d
   hfg_ctx* ctx = df->ctx;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
+  AllocScope alloc_scope(ctx->stream);
   const long long nn = (long long)df->n * df->n;
   int rc = cuda_check(ctx, df->Cd.alloc((size_t)df->n * nocc), "alloc");
   if (rc == HFG_OK) rc = cuda_check(ctx, df->J.alloc(nn), "alloc");

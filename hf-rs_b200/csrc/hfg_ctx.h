@@ -28,6 +28,7 @@ struct PairClass {
 
 struct Launch {
   int la, lb, lc, ld, G;
+  cudaStream_t st = nullptr;  // stream of the entries/prefix allocations
   bool fp32;
   double quartets = 0, prims = 0;  // shell quartets and primitive quartets (after screening) of this launch
   std::vector<JKEntry> entries;
@@ -41,23 +42,44 @@ struct Plan {
   hfg_jk_stats stats{};
 };
 
-// Device buffer owned by the context.
+// Stream on which DevBuf allocations of the current host thread are made
+// (stream-ordered cudaMallocAsync / cudaFreeAsync, so that jobs running on
+// different streams never synchronise the device through cudaFree).  Each
+// C-ABI entry point sets it to its context's stream for its duration.
+extern thread_local cudaStream_t tl_alloc_stream;
+struct AllocScope {
+  cudaStream_t prev;
+  explicit AllocScope(cudaStream_t s) : prev(tl_alloc_stream) { tl_alloc_stream = s; }
+  ~AllocScope() { tl_alloc_stream = prev; }
+};
+
+// Device buffer (stream-ordered when allocated under an AllocScope).
 template <typename T> struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t st = nullptr;
   cudaError_t alloc(size_t count) {
     if (count <= n) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-    if (e == cudaSuccess) n = count;
+    release();
+    st = tl_alloc_stream;
+    cudaError_t e = st ? cudaMallocAsync((void**)&p, count * sizeof(T), st) : cudaMalloc(&p, count * sizeof(T));
+    if (e == cudaSuccess) n = count; else p = nullptr;
     return e;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (st) cudaFreeAsync(p, st); else cudaFree(p);
+    }
     p = nullptr;
     n = 0;
+  }
+  ~DevBuf() { release(); }
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), st(o.st) {
+    o.p = nullptr;
+    o.n = 0;
   }
 };
 

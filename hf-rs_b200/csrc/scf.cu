@@ -171,6 +171,20 @@ void solid_harmonic(int l, int m, std::vector<std::pair<std::array<int, 3>, doub
   }
 }
 
+// cuBLAS / cuSOLVER handles are created once per host thread and device and
+// reused by every SCF that thread runs (handle creation costs milliseconds,
+// which matters for streams of small jobs); each call binds its stream.
+struct ThreadHandles {
+  int device = -1;
+  cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  ~ThreadHandles() {
+    if (blas) cublasDestroy(blas);
+    if (solver) cusolverDnDestroy(solver);
+  }
+};
+thread_local ThreadHandles tl_handles;
+
 struct Scf {
   hfg_ctx* ctx;
   cublasHandle_t blas = nullptr;
@@ -179,10 +193,6 @@ struct Scf {
   DevBuf<double> S, H, T, V, X, W, tmp1, tmp2, evals, work;
   DevBuf<int> info;
   int lwork = 0;
-  ~Scf() {
-    if (blas) cublasDestroy(blas);
-    if (solver) cusolverDnDestroy(solver);
-  }
   int gemm(cublasOperation_t ta, cublasOperation_t tb, int M, int N, int K, double alpha, const double* A, int lda,
            const double* B, int ldb, double beta, double* C, int ldc) {
     const cublasStatus_t s = cublasDgemm(blas, ta, tb, M, N, K, &alpha, A, lda, B, ldb, &beta, C, ldc);
@@ -240,8 +250,18 @@ int scf_setup(hfg_ctx* ctx, const hfg_scf_opts* o, Scf& s, int& m_out) {
   } while (0)
   s.ctx = ctx;
   s.n = n;
-  if (cublasCreate(&s.blas) != CUBLAS_STATUS_SUCCESS) return set_error(ctx, HFG_ERR_CUDA, "cublasCreate");
-  if (cusolverDnCreate(&s.solver) != CUSOLVER_STATUS_SUCCESS) return set_error(ctx, HFG_ERR_CUDA, "cusolverDnCreate");
+  if (tl_handles.device != ctx->device) {
+    if (tl_handles.blas) cublasDestroy(tl_handles.blas);
+    if (tl_handles.solver) cusolverDnDestroy(tl_handles.solver);
+    tl_handles.blas = nullptr;
+    tl_handles.solver = nullptr;
+    if (cublasCreate(&tl_handles.blas) != CUBLAS_STATUS_SUCCESS) return set_error(ctx, HFG_ERR_CUDA, "cublasCreate");
+    if (cusolverDnCreate(&tl_handles.solver) != CUSOLVER_STATUS_SUCCESS)
+      return set_error(ctx, HFG_ERR_CUDA, "cusolverDnCreate");
+    tl_handles.device = ctx->device;
+  }
+  s.blas = tl_handles.blas;
+  s.solver = tl_handles.solver;
   cublasSetStream(s.blas, ctx->stream);
   cusolverDnSetStream(s.solver, ctx->stream);
   const long long nn = (long long)n * n;
@@ -352,6 +372,7 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   auto t_start = std::chrono::steady_clock::now();
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
+  AllocScope alloc_scope(ctx->stream);
   *res = hfg_scf_result{};
   const int n = ctx->n;
   if (o->natom <= 0 || !o->positions || !o->charges)
@@ -653,6 +674,7 @@ extern "C" int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts*
   auto t_start = std::chrono::steady_clock::now();
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
+  AllocScope alloc_scope(ctx->stream);
   *res = hfg_scf_result{};
   const int n = ctx->n;
   double zsum = 0.0;

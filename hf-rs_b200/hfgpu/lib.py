@@ -68,6 +68,24 @@ def convergence_from_tol(tol):
     return tol, max(math.sqrt(tol) * 1e-2, 1e-11), min(max(math.sqrt(tol) * 0.1, 1e-12), 1e-10)
 
 
+class Job(ctypes.Structure):
+    _fields_ = [("basis", HfgBasis), ("natom", ctypes.c_int), ("positions", ctypes.POINTER(ctypes.c_double)),
+                ("charges", ctypes.POINTER(ctypes.c_double)), ("charge", ctypes.c_int),
+                ("multiplicity", ctypes.c_int), ("uhf", ctypes.c_int), ("spherical", ctypes.c_int),
+                ("max_iter", ctypes.c_int), ("energy_tol", ctypes.c_double), ("residual_tol", ctypes.c_double),
+                ("density_tol", ctypes.c_double), ("jk", JKOptions), ("tag", ctypes.c_longlong)]
+
+
+class JobResult(ctypes.Structure):
+    _fields_ = [("tag", ctypes.c_longlong), ("status", ctypes.c_int), ("iterations", ctypes.c_int),
+                ("converged", ctypes.c_int), ("n_ao", ctypes.c_int), ("energy", ctypes.c_double),
+                ("energy_before_refinement", ctypes.c_double), ("submit_ms", ctypes.c_double),
+                ("start_ms", ctypes.c_double), ("end_ms", ctypes.c_double), ("footprint_bytes", ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class JKStats(ctypes.Structure):
     _fields_ = [("quartets_fp64", ctypes.c_double), ("quartets_fp32", ctypes.c_double),
                 ("prim_quartets_fp64", ctypes.c_double), ("prim_quartets_fp32", ctypes.c_double),
@@ -123,6 +141,11 @@ def load_library():
     L.hfg_df_metric.argtypes = [VP, DP]
     L.hfg_df_jk.argtypes = [VP, DP, ctypes.c_int, DP, DP, ctypes.c_int]
     L.hfg_scf_df.argtypes = [VP, VP, ctypes.c_int, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
+    L.hfg_server_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, P(VP)]
+    L.hfg_server_submit.argtypes = [VP, P(Job)]
+    L.hfg_server_poll.argtypes = [VP, P(JobResult), ctypes.c_int, P(ctypes.c_int), ctypes.c_int]
+    L.hfg_server_stats.argtypes = [VP, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_longlong)]
+    L.hfg_server_destroy.argtypes = [VP]
     L.hfg_scf.argtypes = [VP, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     _lib = L
     return L
@@ -345,6 +368,60 @@ class DFTensor:
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
             self.lib.hfg_df_destroy(self.h)
+            self.h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """hfg_server: continuous admission of SCF jobs onto worker slots."""
+
+    def __init__(self, device=0, slots=8, hbm_budget_bytes=64 << 30):
+        self.lib = load_library()
+        h = VP()
+        rc = self.lib.hfg_server_create(device, slots, hbm_budget_bytes, ctypes.byref(h))
+        if rc != 0:
+            raise HfgError(rc, "hfg_server_create failed")
+        self.h = h
+
+    def submit(self, basis, charge=0, multiplicity=1, uhf=False, spherical=False, tol=1e-10, max_iter=100,
+               jk=None, tag=0):
+        pos = np.ascontiguousarray(basis.positions())
+        chg = np.ascontiguousarray(basis.nuclear_charges())
+        j = Job()
+        j.basis = HfgBasis(basis.n, _dp(basis.center), _ip(basis.lxyz), _ip(basis.atom), _ip(basis.prim_off),
+                           _dp(basis.exps), _dp(basis.coefs))
+        j.natom = len(chg)
+        j.positions, j.charges = _dp(pos), _dp(chg)
+        j.charge, j.multiplicity, j.uhf, j.spherical = charge, multiplicity, int(uhf), int(spherical)
+        j.max_iter = max_iter
+        j.energy_tol, j.residual_tol, j.density_tol = convergence_from_tol(tol)
+        j.jk = jk or JKOptions.make()
+        j.tag = tag
+        rc = self.lib.hfg_server_submit(self.h, ctypes.byref(j))  # inputs copied before return
+        if rc != 0:
+            raise HfgError(rc, "hfg_server_submit failed")
+
+    def poll(self, wait=False, max_results=256):
+        buf = (JobResult * max_results)()
+        n = ctypes.c_int()
+        rc = self.lib.hfg_server_poll(self.h, buf, max_results, ctypes.byref(n), int(wait))
+        if rc != 0:
+            raise HfgError(rc, "hfg_server_poll failed")
+        return [buf[i].as_dict() for i in range(n.value)]
+
+    def stats(self):
+        p, r, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        self.lib.hfg_server_stats(self.h, ctypes.byref(p), ctypes.byref(r), ctypes.byref(b))
+        return {"pending": p.value, "running": r.value, "in_use_bytes": b.value}
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.hfg_server_destroy(self.h)
             self.h = VP()
 
     def __del__(self):

@@ -226,6 +226,46 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* opts, hfg_scf_result* result, doub
 int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts* opts, hfg_scf_result* result, double* P,
                double* F, double* J, double* K);
 
+/* ---- Serving: a request loop for streams of SCF jobs (no hf-rs counterpart;
+   each job runs the hfg_scf equivalent of run_scf_in_space_with_convergence /
+   run_uhf_in_space_with_convergence). ---- */
+typedef struct {
+  hfg_basis basis;          /* copied at submit */
+  int natom;
+  const double* positions;  /* [natom][3] bohr, copied */
+  const double* charges;    /* [natom], copied */
+  int charge, multiplicity, uhf, spherical;
+  int max_iter;
+  double energy_tol, residual_tol, density_tol;
+  hfg_jk_opts jk;
+  long long tag;            /* caller's identifier, returned with the result */
+} hfg_job;
+
+typedef struct {
+  long long tag;
+  int status, iterations, converged, n_ao;
+  double energy, energy_before_refinement;
+  double submit_ms, start_ms, end_ms; /* since hfg_server_create */
+  long long footprint_bytes;
+} hfg_job_result;
+
+typedef struct hfg_server hfg_server;
+
+/* `slots` worker slots (host threads with their own CUDA streams) on one
+   device; jobs are admitted first in, first out when a slot is free and their
+   estimated device footprint fits in `hbm_budget_bytes` minus the running
+   jobs' footprints. */
+int hfg_server_create(int device, int slots, long long hbm_budget_bytes, hfg_server** out);
+/* Queue a job (non-blocking; inputs are copied).  HFG_ERR_OOM if the job
+   alone exceeds the budget. */
+int hfg_server_submit(hfg_server* server, const hfg_job* job);
+/* Up to `max` completed jobs; with wait_for_one, blocks until one completes
+   or nothing is pending or running. */
+int hfg_server_poll(hfg_server* server, hfg_job_result* out, int max, int* n_out, int wait_for_one);
+int hfg_server_stats(hfg_server* server, int* pending, int* running, long long* in_use_bytes);
+/* Finishes the queued jobs, then stops the workers. */
+int hfg_server_destroy(hfg_server* server);
+
 /* Measured FMA-pipe peak of the device in TFLOP/s (FP64 when fp32 == 0):
    independent FMA chains in registers on every SM.  The roofline
    denominator of the ERI kernels, which are bound by these pipes. */

@@ -1,0 +1,30 @@
+"""Serving loop: every job's result is the same alone and in a mix, and
+admission respects the device-memory budget."""
+import pytest
+
+from hfgpu.serve import build_inputs, make_stream, run_stream, summarize
+
+pytestmark = pytest.mark.gpu
+
+
+def test_results_same_alone_and_in_the_mix():
+    jobs = make_stream(12, rate=1000.0, max_waters=4, seed=7)
+    inputs = build_inputs(jobs)
+    alone, _ = run_stream(jobs, slots=1, budget_bytes=8 << 30, honour_arrivals=False, inputs=inputs)
+    mixed, span = run_stream(jobs, slots=6, budget_bytes=8 << 30, honour_arrivals=False, inputs=inputs)
+    assert all(r["status"] == 0 and r["converged"] for r in alone + mixed)
+    for a, m in zip(alone, mixed):
+        assert abs(a["energy"] - m["energy"]) < 1e-10, (a["tag"], a["energy"], m["energy"])
+    s = summarize(mixed, span)
+    assert s["jobs"] == 12 and s["failed"] == 0
+
+
+def test_admission_by_footprint_limits_concurrency():
+    jobs = make_stream(6, rate=1000.0, max_waters=3, seed=9)
+    inputs = build_inputs(jobs)
+    res, _ = run_stream(jobs, slots=6, budget_bytes=24 << 20, honour_arrivals=False, inputs=inputs)
+    # with a 24 MiB budget the jobs (each several MiB) cannot all run at once:
+    # some job must start only after another ended
+    starts = sorted((r["start_ms"], r["end_ms"]) for r in res)
+    assert any(s2 >= e1 for (s1, e1), (s2, e2) in zip(starts, starts[1:]))
+    assert all(r["status"] == 0 for r in res)
