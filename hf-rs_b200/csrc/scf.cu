@@ -23,6 +23,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <map>
+#include <memory>
 #include <vector>
 
 #include "hfg_ctx.h"
@@ -346,6 +348,236 @@ int scf_setup(hfg_ctx* ctx, const hfg_scf_opts* o, Scf& s, int& m_out) {
 #undef CK
 #undef RK
 }
+
+// ---------------------------------------------------------------------------
+// Superposition of atomic densities (src/sad.rs:24-259): for each element
+// (keyed by nuclear charge and its basis functions) a spin-averaged atomic
+// RHF with fractional occupations -- degenerate levels (within 1e-6) share
+// their electrons equally -- converged with CDIIS(8) and 0.5 damping for the
+// first five iterations (|dE| < 1e-11, rmsd(D - D_next) < 1e-9, max|FDS - SDF|
+// < 1e-8).  Hydrogen's atomic Fock operator is H alone.  Results are cached
+// per element; the molecular guess is their block-diagonal superposition
+// rescaled to Tr(PS) = N.
+std::mutex g_sad_mu;
+std::map<std::vector<double>, std::vector<double>> g_sad_cache;
+
+std::vector<double> occupations(const std::vector<double>& eps, double nel) {
+  std::vector<double> occ(eps.size(), 0.0);
+  double left = nel;
+  size_t i = 0;
+  while (i < eps.size() && left > 1e-12) {
+    size_t end = i + 1;
+    while (end < eps.size() && std::fabs(eps[end] - eps[i]) < 1e-6) ++end;
+    const double pop = std::min(left, 2.0 * (double)(end - i));
+    for (size_t k = i; k < end; ++k) occ[k] = pop / (double)(end - i);
+    left -= pop;
+    i = end;
+  }
+  return occ;
+}
+
+__global__ void scale_cols_by(double* __restrict__ C, const double* __restrict__ w, int n, int m) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (long long)n * m) C[t] *= w[t / n];
+}
+
+// Atomic fractional HF density of the functions [f0, f1) of `ctx` (one atom).
+int atomic_density(hfg_ctx* ctx, int f0, int f1, double Z, std::vector<double>& out) {
+  const int n = f1 - f0;
+  // the atom's functions at the origin, as an hfg_basis
+  std::vector<double> center(3 * n, 0.0), exps, coefs;
+  std::vector<int> lxyz(3 * n), atom(n, 0), off(1, 0);
+  for (const auto& sh : ctx->shells) {
+    if (sh.ao < f0 || sh.ao >= f1) continue;
+    std::vector<std::array<int, 3>> comps;
+    if (sh.l == 2) comps = {{2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+    else
+      for (int lx = sh.l; lx >= 0; --lx)
+        for (int ly = sh.l - lx; ly >= 0; --ly) comps.push_back({lx, ly, sh.l - lx - ly});
+    for (size_t c = 0; c < comps.size(); ++c) {
+      const int f = sh.ao + (int)c - f0;
+      for (int k = 0; k < 3; ++k) lxyz[3 * f + k] = comps[c][k];
+      const double sc = 1.0 / std::sqrt(dfact(2 * comps[c][0] - 1) * dfact(2 * comps[c][1] - 1) * dfact(2 * comps[c][2] - 1));
+      for (int q = 0; q < sh.K; ++q) {
+        exps.push_back(ctx->exps[sh.prim_off + q]);
+        coefs.push_back(ctx->coefs[sh.prim_off + q] * sc);
+      }
+      off.push_back((int)exps.size());
+    }
+  }
+  hfg_basis b{n, center.data(), lxyz.data(), atom.data(), off.data(), exps.data(), coefs.data()};
+  hfg_ctx* ac = nullptr;
+  int rc = hfg_ctx_create(&b, ctx->device, ctx->stream, &ac);
+  if (rc != HFG_OK) {
+    if (ac) hfg_ctx_destroy(ac);
+    return set_error(ctx, rc, "SAD atomic context");
+  }
+  std::unique_ptr<hfg_ctx, int (*)(hfg_ctx*)> guard(ac, hfg_ctx_destroy);
+  hfg_scf_opts o;
+  hfg_scf_opts_default(&o);
+  const double origin[3] = {0.0, 0.0, 0.0};
+  o.natom = 1;
+  o.positions = origin;
+  o.charges = &Z;
+  Scf s;
+  int m = 0;
+  rc = scf_setup(ac, &o, s, m);
+  if (rc != HFG_OK) return set_error(ctx, rc, "SAD setup: " + ac->err);
+  const long long nn = (long long)n * n;
+  DevBuf<double> D, Dn, F, J, K, Fp, C, E, Fh, Eh, Fx, wv;
+  auto ok = [&](cudaError_t e) { return e == cudaSuccess; };
+  if (!ok(D.alloc(nn)) || !ok(Dn.alloc(nn)) || !ok(F.alloc(nn)) || !ok(J.alloc(nn)) || !ok(K.alloc(nn)) ||
+      !ok(Fp.alloc(nn)) || !ok(C.alloc(nn)) || !ok(E.alloc(nn)) || !ok(Fh.alloc(8 * nn)) || !ok(Eh.alloc(8 * nn)) ||
+      !ok(Fx.alloc(nn)) || !ok(wv.alloc(n)))
+    return set_error(ctx, HFG_ERR_OOM, "SAD buffers");
+  cudaStream_t st = ac->stream;
+  std::vector<double> eps(m);
+  // density from a Fock-like matrix with fractional occupations
+  auto dens = [&](const double* Fm, double* Dm) -> int {
+    if (s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, m, n, 1.0, Fm, n, s.X.p, n, 0.0, s.tmp1.p, n)) return HFG_ERR_CUDA;
+    if (s.gemm(CUBLAS_OP_T, CUBLAS_OP_N, m, m, n, 1.0, s.X.p, n, s.tmp1.p, n, 0.0, Fp.p, m)) return HFG_ERR_CUDA;
+    if (s.eigh(Fp.p, s.evals.p, m)) return HFG_ERR_CUDA;
+    if (s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, 1.0, s.X.p, n, Fp.p, m, 0.0, C.p, n)) return HFG_ERR_CUDA;
+    cudaMemcpyAsync(eps.data(), s.evals.p, m * 8, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    std::vector<double> occ = occupations(eps, Z);
+    for (auto& v : occ) v = std::sqrt(v);
+    cudaMemcpyAsync(wv.p, occ.data(), m * 8, cudaMemcpyHostToDevice, st);
+    scale_cols_by<<<nblk((long long)n * m), 256, 0, st>>>(C.p, wv.p, n, m);
+    return s.gemm(CUBLAS_OP_N, CUBLAS_OP_T, n, n, m, 1.0, C.p, n, C.p, n, 0.0, Dm, n);
+  };
+  auto fock = [&](const double* Dm) -> int {
+    cudaMemcpyAsync(F.p, s.H.p, nn * 8, cudaMemcpyDeviceToDevice, st);
+    if (std::fabs(Z - 1.0) < 1e-12) return HFG_OK;
+    hfg_jk_opts jo;
+    hfg_jk_opts_default(&jo);
+    int r = jk_device_locked(ac, &jo, 1, Dm, Dm, J.p, K.p);
+    if (r != HFG_OK) return r;
+    axpby_kernel<<<nblk(nn), 256, 0, st>>>(F.p, J.p, 1.0, 1.0, nn);
+    axpby_kernel<<<nblk(nn), 256, 0, st>>>(F.p, K.p, -0.5, 1.0, nn);
+    return HFG_OK;
+  };
+  if ((rc = dens(s.H.p, D.p)) != HFG_OK) return set_error(ctx, rc, "SAD");
+  double prev = INFINITY;
+  std::vector<int> slot;
+  std::vector<double> Bm;
+  int count = 0;
+  for (int it = 1; it <= 200; ++it) {
+    if ((rc = fock(D.p)) != HFG_OK) return set_error(ctx, rc, "SAD Fock");
+    const double e = 0.5 * (s.dot(D.p, s.H.p, nn) + s.dot(D.p, F.p, nn));
+    if ((rc = dens(F.p, Dn.p)) != HFG_OK) return set_error(ctx, rc, "SAD");
+    // error FDS - SDF and rmsd(D - Dn)
+    s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, F.p, n, D.p, n, 0.0, s.tmp1.p, n);
+    s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, s.tmp1.p, n, s.S.p, n, 0.0, s.T.p, n);
+    antisym_kernel<<<nblk(nn), 256, 0, st>>>(s.T.p, E.p, n);
+    const double err = s.maxabs(E.p, nn);
+    cudaMemcpyAsync(s.tmp1.p, D.p, nn * 8, cudaMemcpyDeviceToDevice, st);
+    axpby_kernel<<<nblk(nn), 256, 0, st>>>(s.tmp1.p, Dn.p, -1.0, 1.0, nn);
+    double nr = 0.0;
+    cublasDnrm2(s.blas, (int)nn, s.tmp1.p, 1, &nr);
+    const double rmsd = nr / std::sqrt((double)nn);
+    if (std::fabs(e - prev) < 1e-11 && rmsd < 1e-9 && err < 1e-8) {
+      out.resize(nn);
+      cudaMemcpyAsync(out.data(), Dn.p, nn * 8, cudaMemcpyDeviceToHost, st);
+      cudaStreamSynchronize(st);
+      return HFG_OK;
+    }
+    prev = e;
+    int sl;
+    if (count < 8) {
+      sl = count++;
+      slot.push_back(sl);
+    } else {
+      sl = slot.front();
+      slot.erase(slot.begin());
+      slot.push_back(sl);
+    }
+    cudaMemcpyAsync(Fh.p + (long long)sl * nn, F.p, nn * 8, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(Eh.p + (long long)sl * nn, E.p, nn * 8, cudaMemcpyDeviceToDevice, st);
+    const int k = (int)slot.size();
+    std::vector<double> Bn((size_t)k * k);
+    const int kprev = (int)std::sqrt((double)Bm.size());
+    for (int i = 0; i < k - 1; ++i)
+      for (int j = 0; j < k - 1; ++j) Bn[(size_t)i * k + j] = Bm[(size_t)(kprev - (k - 1) + i) * kprev + kprev - (k - 1) + j];
+    for (int i = 0; i < k; ++i) {
+      const double d = s.dot(Eh.p + (long long)slot[i] * nn, Eh.p + (long long)sl * nn, nn);
+      Bn[(size_t)i * k + (k - 1)] = Bn[(size_t)(k - 1) * k + i] = d;
+    }
+    Bm = Bn;
+    const double* Fuse = F.p;
+    if (k >= 2) {
+      const int dim = k + 1;
+      std::vector<double> A((size_t)dim * dim, 0.0), x(dim, 0.0);
+      for (int i = 0; i < k; ++i) {
+        for (int j = 0; j < k; ++j) A[(size_t)i * dim + j] = Bm[(size_t)i * k + j];
+        A[(size_t)i * dim + k] = A[(size_t)k * dim + i] = -1.0;
+      }
+      x[k] = -1.0;
+      if (solve_small(A, x, dim)) {
+        cudaMemsetAsync(Fx.p, 0, nn * 8, st);
+        for (int i = 0; i < k; ++i)
+          axpby_kernel<<<nblk(nn), 256, 0, st>>>(Fx.p, Fh.p + (long long)slot[i] * nn, x[i], 1.0, nn);
+        Fuse = Fx.p;
+      }
+    }
+    if ((rc = dens(Fuse, Dn.p)) != HFG_OK) return set_error(ctx, rc, "SAD");
+    if (it <= 5) axpby_kernel<<<nblk(nn), 256, 0, st>>>(D.p, Dn.p, 0.5, 0.5, nn);
+    else cudaMemcpyAsync(D.p, Dn.p, nn * 8, cudaMemcpyDeviceToDevice, st);
+  }
+  return set_error(ctx, HFG_ERR_SCF, "fractional atomic HF did not converge");
+}
+
+// SAD density of the molecule into dP (device, n x n), rescaled to nel.
+int sad_guess(hfg_ctx* ctx, const hfg_scf_opts* o, Scf& s, double nel, double* dP) {
+  const int n = ctx->n;
+  std::vector<double> P((size_t)n * n, 0.0);
+  // functions of each atom (consecutive shells of one atom index)
+  std::map<int, std::pair<int, int>> range;
+  for (const auto& sh : ctx->shells) {
+    auto it = range.find(sh.atom);
+    const int f1 = sh.ao + (sh.l + 1) * (sh.l + 2) / 2;
+    if (it == range.end()) range[sh.atom] = {sh.ao, f1};
+    else {
+      if (sh.ao != it->second.second) return set_error(ctx, HFG_ERR_INVALID_INPUT, "atom functions not contiguous");
+      it->second.second = f1;
+    }
+  }
+  for (auto& kv : range) {
+    const int a = kv.first, f0 = kv.second.first, f1 = kv.second.second;
+    if (a < 0 || a >= o->natom) return set_error(ctx, HFG_ERR_INVALID_INPUT, "atom index out of range");
+    const double Z = o->charges[a];
+    std::vector<double> key{Z};
+    for (const auto& sh : ctx->shells)
+      if (sh.ao >= f0 && sh.ao < f1) {
+        key.push_back(sh.l);
+        for (int q = 0; q < sh.K; ++q) {
+          key.push_back(ctx->exps[sh.prim_off + q]);
+          key.push_back(ctx->coefs[sh.prim_off + q]);
+        }
+      }
+    std::vector<double> Da;
+    {
+      std::lock_guard<std::mutex> lk(g_sad_mu);
+      auto it = g_sad_cache.find(key);
+      if (it != g_sad_cache.end()) Da = it->second;
+    }
+    if (Da.empty()) {
+      const int rc = atomic_density(ctx, f0, f1, Z, Da);
+      if (rc != HFG_OK) return rc;
+      std::lock_guard<std::mutex> lk(g_sad_mu);
+      g_sad_cache[key] = Da;
+    }
+    const int na = f1 - f0;
+    for (int i = 0; i < na; ++i)
+      for (int j = 0; j < na; ++j) P[(size_t)(f0 + i) * n + f0 + j] = Da[(size_t)i * na + j];
+  }
+  cudaMemcpyAsync(dP, P.data(), P.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+  const double el = s.dot(dP, s.S.p, (long long)n * n);
+  if (el <= 1e-12) return set_error(ctx, HFG_ERR_SCF, "zero SAD population");
+  const double scale = nel / el;
+  cublasDscal(s.blas, n * n, &scale, dP, 1);
+  return HFG_OK;
+}
 }  // namespace
 }  // namespace hfg
 
@@ -491,8 +723,26 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   };
   const long long elen_eff = m < n ? elen : nn;
 
-  // initial guess: core Hamiltonian orbitals (the fallback of src/scf.rs:464-470)
-  for (int sp = 0; sp < nspin; ++sp) RK(diag(s.H.p, C.p + sp * (long long)n * m, P.p + sp * nn, s.evals.p, nocc[sp]));
+  // initial guess (src/scf.rs:452-471 for RHF, :742-751 for UHF): the SAD
+  // density (RHF starts from it; UHF from the orbitals of its Fock matrix),
+  // or core Hamiltonian orbitals
+  if (o->guess == 0) {
+    RK(sad_guess(ctx, o, s, (double)nel, Ptot));
+    if (!uhf) {
+      CK(cudaMemcpyAsync(P.p, Ptot, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+      // Fock of the SAD density with RHF weights, then its orbitals
+      hfg_jk_opts j64 = o->jk;
+      j64.precision = HFG_FP64;
+      RK(jk_device_locked(ctx, &j64, 1, Ptot, Ptot, J.p, K.p));
+      CK(cudaMemcpyAsync(F.p, s.H.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+      axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(F.p, J.p, 1.0, 1.0, nn);
+      axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(F.p, K.p, -0.5, 1.0, nn);
+      for (int sp = 0; sp < 2; ++sp) RK(diag(F.p, C.p + sp * (long long)n * m, P.p + sp * nn, s.evals.p, nocc[sp]));
+    }
+  } else {
+    for (int sp = 0; sp < nspin; ++sp) RK(diag(s.H.p, C.p + sp * (long long)n * m, P.p + sp * nn, s.evals.p, nocc[sp]));
+  }
 
   const bool mixed = o->jk.precision == HFG_MIXED;
   hfg_jk_opts jo = o->jk;

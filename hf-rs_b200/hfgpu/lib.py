@@ -48,7 +48,7 @@ class SCFOptions(ctypes.Structure):
                 ("multiplicity", ctypes.c_int), ("uhf", ctypes.c_int), ("spherical", ctypes.c_int),
                 ("max_iter", ctypes.c_int), ("energy_tol", ctypes.c_double), ("residual_tol", ctypes.c_double),
                 ("density_tol", ctypes.c_double), ("jk", JKOptions), ("refine_iters", ctypes.c_int),
-                ("diis_size", ctypes.c_int), ("verbose", ctypes.c_int)]
+                ("diis_size", ctypes.c_int), ("verbose", ctypes.c_int), ("guess", ctypes.c_int)]
 
 
 class SCFResult(ctypes.Structure):
@@ -254,7 +254,7 @@ class Context:
         return Fa, Fb
 
     def scf(self, charge=0, multiplicity=1, uhf=False, spherical=False, tol=1e-10, max_iter=100, jk=None,
-            refine_iters=2, verbose=False, want=("P", "F")):
+            refine_iters=2, verbose=False, want=("P", "F"), guess="sad"):
         """Device SCF (hfg_scf) for the context's molecule; returns a dict."""
         b = self.basis
         o = SCFOptions()
@@ -270,6 +270,7 @@ class Context:
         o.jk = jk or JKOptions.make()
         o.refine_iters = refine_iters
         o.verbose = int(verbose)
+        o.guess = 0 if guess == "sad" else 1
         n = self.n
         ns = 2 if uhf else 1
         P = np.zeros((ns, n, n)) if "P" in want else None

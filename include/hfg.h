@@ -187,6 +187,8 @@ typedef struct {
   int refine_iters;
   int diis_size;           /* CDIIS subspace (hf-rs: 8, src/scf.rs:479) */
   int verbose;             /* iteration table on stderr */
+  int guess;               /* 0: superposition of atomic densities (hf-rs's default, src/sad.rs),
+                              1: core Hamiltonian */
 } hfg_scf_opts;
 
 typedef struct {
@@ -207,7 +209,9 @@ void hfg_scf_opts_default(hfg_scf_opts* opts);
  * Stands in for run_scf_in_space_with_convergence (src/scf.rs:410-627) and
  * run_uhf_in_space_with_convergence (src/scf.rs:691-979) with CDIIS: a
  * direct SCF whose one-electron integrals, Fock builds, DIIS and
- * diagonalisations all run on the device.  Initial guess: core Hamiltonian.
+ * diagonalisations all run on the device.  Initial guess as hf-rs: the
+ * superposition of cached atomic fractional-occupation HF densities
+ * (src/sad.rs:56-259), or the core Hamiltonian on request.
  * Optional outputs (NULL to skip), row-major: P and F (nspin x n x n),
  * C (nspin x n x n_mo, Cartesian rows), orbital energies (nspin x n_mo).
  * Returns HFG_ERR_SCF if not converged within max_iter (results still set).

@@ -24,6 +24,17 @@ def test_scf_energies_match_golden(golden_dir):
         ctx.close()
 
 
+def test_sad_guess_and_cdiis_follow_the_reference_iterations():
+    # same SAD guess and CDIIS as hf-rs -> same iteration history as the oracle
+    for name in ("sto-3g", "6-31g*", "cc-pvdz"):
+        atoms = water_cluster(2)
+        ctx = Context(CartesianBasis.build(atoms, name))
+        r = ctx.scf(tol=1e-10, spherical=(name == "cc-pvdz"))
+        ref = O.rhf(atoms, O.build_basis(atoms, O.load_basis(name)), tol=1e-10, spherical=(name == "cc-pvdz"))
+        assert r["converged"] and abs(r["energy"] - ref["energy"]) <= 1e-10
+        assert abs(r["iterations"] - ref["iterations"]) <= 1, (name, r["iterations"], ref["iterations"])
+
+
 def test_water_ccpvdz_spherical_golden(golden_dir):
     # hf-rs tests/spherical_basis_test.rs:135-166 (24 retained MOs, 1e-9 Eh)
     d = json.load(open(os.path.join(golden_dir, "water_ccpvdz.json")))
