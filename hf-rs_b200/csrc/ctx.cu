@@ -358,7 +358,9 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     const PairClass& B = ctx->classes[cb];
     for (int ck = 0; ck <= cb; ++ck) {
       const PairClass& Kc = ctx->classes[ck];
-      const int qpw = 32;
+      const long kk = (long)B.Ka * B.Kb * Kc.Ka * Kc.Kb;
+      const int G = choose_group(B.la, B.lb, Kc.la, Kc.lb, kk);
+      const int qpw = 32 / G;
       const double w = wmd_flops(B.la, B.lb, Kc.la, Kc.lb);
       for (int i = B.first; i < B.first + B.count; ++i) {
         const double qi = Q[i];
@@ -385,7 +387,7 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
         for (int r = 0; r < 2; ++r) {
           const int a0 = ranges[r][0], a1 = ranges[r][1];
           if (a1 <= a0) continue;
-          Launch& L = get_launch(B.la, B.lb, Kc.la, Kc.lb, 1, r == 1);
+          Launch& L = get_launch(B.la, B.lb, Kc.la, Kc.lb, G, r == 1);
           L.entries.push_back({i, Kc.first + a0, Kc.first + a1, 0});
           L.prefix.push_back(L.prefix.back() + (a1 - a0 + qpw - 1) / qpw);
           const double nq = a1 - a0;
@@ -432,7 +434,7 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     HFG_CUDA(ctx, cudaMemsetAsync(cnt.p, 0, plan->launches.size() * 8, ctx->stream));
     for (size_t l = 0; l < plan->launches.size(); ++l) {
       const Launch& L = plan->launches[l];
-      HFG_CUDA(ctx, launch_count(L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1], ctx->d_pairs.p,
+      HFG_CUDA(ctx, launch_count(L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1], L.G, ctx->d_pairs.p,
                                  ctx->d_pbound.p, prim_eps, cnt.p + l, ctx->stream));
     }
     std::vector<unsigned long long> h(plan->launches.size());
@@ -524,7 +526,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
     a.prefix = L.d_prefix;
     a.nentries = (int)L.prefix[0];
     a.nwarps = L.prefix[1];
-    HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.fp32, a, ctx->stream));
+    HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.G, L.fp32, a, ctx->stream));
     if (profile) cudaEventRecord(ev[l + 1], ctx->stream);
   }
   if (profile) {
@@ -535,8 +537,8 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
       cudaEventElapsedTime(&ms, ev[l], ev[l + 1]);
       tot += ms;
       const Launch& L = plan->launches[l];
-      fprintf(stderr, "hfg-profile (%d%d|%d%d) %s entries %8lld warps %10lld quartets %.3e prims %.3e  %9.3f ms  %.3e prim/s\n",
-              L.la, L.lb, L.lc, L.ld, L.fp32 ? "fp32" : "fp64", L.prefix[0], L.prefix[1], L.quartets, L.prims, ms,
+      fprintf(stderr, "hfg-profile (%d%d|%d%d) G%-2d %s entries %8lld warps %10lld quartets %.3e prims %.3e  %9.3f ms  %.3e prim/s\n",
+              L.la, L.lb, L.lc, L.ld, L.G, L.fp32 ? "fp32" : "fp64", L.prefix[0], L.prefix[1], L.quartets, L.prims, ms,
               L.prims / (ms * 1e-3));
     }
     fprintf(stderr, "hfg-profile total %.3f ms\n", tot);

@@ -241,8 +241,14 @@ constexpr int kChunk = 8;
 #define HFG_JK_MIN_BLOCKS 2
 #endif
 
-template <int LA, int LB, int LC, int LD, typename T, int NS>
+// G lanes per shell quartet (G = 1: one quartet per lane).  With G > 1 the
+// lanes of a group take the quartet's ket primitive pairs round-robin (they
+// are sorted by bound, so neighbouring lanes see similar screening), all
+// walk the shared bra primitive pairs, and the group reduces its
+// accumulators with shuffles before one lane digests the block.
+template <int LA, int LB, int LC, int LD, typename T, int NS, int G>
 __global__ void __launch_bounds__(256, HFG_JK_MIN_BLOCKS) jk_kernel(const JKLaunchArgs a) {
+  constexpr int QPW = 32 / G;
   using C = EriClass<LA, LB, LC, LD>;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -264,14 +270,15 @@ __global__ void __launch_bounds__(256, HFG_JK_MIN_BLOCKS) jk_kernel(const JKLaun
         next = a.prefix[e + 1];
       }
       const JKEntry ent = a.entries[e];
-      const int kidx = ent.k_lo + (int)(warp - a.prefix[e]) * 32 + lane;
+      const int grp = lane / G, gl = lane - grp * G;
+      const int kidx = ent.k_lo + (int)(warp - a.prefix[e]) * QPW + grp;
       const bool active = kidx < ent.k_hi;
       const PairInfo bra = a.pairs[ent.bra];
       const PairInfo ket = a.pairs[active ? kidx : ent.k_lo];
       // the next task usually continues this entry: touch its ket pair now
-      if (warp + 1 < t1 && kidx + 32 < ent.k_hi) (void)__ldg(&a.pairs[kidx + 32].pp_off);
+      if (warp + 1 < t1 && kidx + QPW < ent.k_hi) (void)__ldg(&a.pairs[kidx + QPW].pp_off);
       DBlocks<LA, LB, LC, LD, NS> dblk;
-      if (active) dblk.load(bra, ket, a);
+      if (active && gl == 0) dblk.load(bra, ket, a);
 
       T acc[C::NACC];
 #pragma unroll
@@ -299,14 +306,27 @@ __global__ void __launch_bounds__(256, HFG_JK_MIN_BLOCKS) jk_kernel(const JKLaun
             if ((double)kb[mid] * bmax >= eps) nke = mid + 1; else hi = mid;
           }
         }
-        Rec Qn = kr[0];
-        for (int ik = 0; ik < nke; ++ik) {
+        Rec Qn = kr[gl < nk ? gl : 0];
+        for (int ik = gl; ik < nke; ik += G) {
           const Rec Q = Qn;
-          if (ik + 1 < nke) Qn = kr[ik + 1];
+          if (ik + G < nke) Qn = kr[ik + G];
           const double qb = kb[ik];
           const T QCx = -Q.bp * kABx, QCy = -Q.bp * kABy, QCz = -Q.bp * kABz;
-          Rec P = br[0];
-          for (int ib = 0; ib < nb; ++ib) {
+          int ib = 0;
+          if constexpr (C::NACC <= 9) {
+            // two independent primitive quartets per step (bra primitive pairs
+            // are sorted by bound: if the second survives, so does the first)
+            for (; ib + 1 < nb; ib += 2) {
+              if ((double)bb[ib + 1] * qb < eps) break;
+              const Rec P0 = br[ib], P1 = br[ib + 1];
+              prim_quartet<LA, LB, LC, LD, T>(acc, P0.p, P0.inv_p, P0.kp, -P0.bp * bABx, -P0.bp * bABy,
+                                              -P0.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
+              prim_quartet<LA, LB, LC, LD, T>(acc, P1.p, P1.inv_p, P1.kp, -P1.bp * bABx, -P1.bp * bABy,
+                                              -P1.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
+            }
+          }
+          Rec P = br[ib < nb ? ib : 0];
+          for (; ib < nb; ++ib) {
             const Rec Pn = br[ib + 1 < nb ? ib + 1 : ib];
             if ((double)bb[ib] * qb < eps) break;
             prim_quartet<LA, LB, LC, LD, T>(acc, P.p, P.inv_p, P.kp, -P.bp * bABx, -P.bp * bABy, -P.bp * bABz, Q.p,
@@ -315,8 +335,15 @@ __global__ void __launch_bounds__(256, HFG_JK_MIN_BLOCKS) jk_kernel(const JKLaun
           }
         }
       }
+      if (G > 1) {
+#pragma unroll
+        for (int x = 0; x < C::NACC; ++x) {
+#pragma unroll
+          for (int off = G / 2; off > 0; off >>= 1) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], off);
+        }
+      }
       double jab[NAB];
-      if (active) {
+      if (active && gl == 0) {
         T out[C::NOUT];
         C::hrr(acc, out, (T)bra.ABx, (T)bra.ABy, (T)bra.ABz, (T)ket.ABx, (T)ket.ABy, (T)ket.ABz);
         double deg = 1.0;
