@@ -30,7 +30,10 @@ sys.path.insert(0, os.path.join(ROOT, "hf-rs_b200"))
 
 METRIC = "fock_builds_per_s"
 UNIT = "Fock builds/s"
-WORKLOAD = "(H2O)64 cc-pVDZ direct RHF Fock build (J+K), 1600 Cartesian AOs, Schwarz 1e-12"
+
+
+def workload(waters, n_ao):
+    return "(H2O)%d cc-pVDZ direct RHF Fock build (J+K), %d Cartesian AOs, Schwarz 1e-12" % (waters, n_ao)
 SCHWARZ = 1e-12
 PRIM = 1e-15
 MIXED = 1e-7
@@ -45,6 +48,10 @@ def parse():
     ap.add_argument("--waters", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-jobs", type=int, default=24)
+    ap.add_argument("--serve-max-waters", type=int, default=16)
+    ap.add_argument("--df-waters", type=int, default=0, help="also time DF J/K on (H2O)_n (0: skip)")
     return ap.parse_args()
 
 
@@ -230,7 +237,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD + ", CPU restatement of hf-rs (McMurchie-Davidson, contract_jk)",
+            "config": {"workload": workload(args.waters, 25 * args.waters) + ", CPU restatement of hf-rs (McMurchie-Davidson, contract_jk)",
                        "parallelism": "openmp-%d" % threads},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": "%d random bra shell-pair rows per step (~%.0f s of CPU work), scaled by "
@@ -377,21 +384,85 @@ def run_ours(args):
                              "total McMurchie-Davidson flops (%.3e per build)" % (nrows, dt, cw.total)}
         except Exception as exc:  # the CPU leg must not hide the GPU result
             cpu = {"unavailable": str(exc)[:200]}
+    serving = None
+    if world == 1 and not args.no_serve:
+        serving = measure_serving(args)
+    dfres = None
+    if world == 1 and args.df_waters > 0:
+        dfres = measure_df(args, torch)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_mixed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32-mixed", "data": "synthetic",
-            "config": {"workload": WORKLOAD + ", mixed precision (FP32 below Q_ab*Q_cd < %g), primitive "
+            "config": {"workload": workload(args.waters, n) + ", mixed precision (FP32 below Q_ab*Q_cd < %g), primitive "
                                               "screening %g" % (MIXED, PRIM),
                        "n_ao": n, "waters": args.waters, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "flushed (256 MB write) before every timed step"},
             "fp64": {"value": value_fp64, "unit": UNIT, "ms_per_step": tot_fp64 / args.steps,
                      "wmd_flops": stats_fp64["wmd_flops_fp64"]},
             "mixed_over_fp64": value / value_fp64, "jk_max_abs_diff_mixed_vs_fp64": jk_diff,
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
-            "gpu_launches": args.steps * 2 * (stats_mixed["launches"] + 2) + args.steps * (stats_fp64["launches"] + 2)}
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck, "serving": serving, "df": dfres,
+            # per build: the plan's J/K launches plus two symmetrisation kernels;
+            # timed: K mixed builds, K FP64 builds and K end-to-end mixed builds
+            "gpu_launches": args.steps * (stats_mixed["launches"] + 2) * (1 if e2e is None else 2)
+            + args.steps * (stats_fp64["launches"] + 2)}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def measure_serving(args):
+    """Served SCF stream vs sequential plain solves on a bounded sample of the
+    seeded job stream (first `serve_jobs` jobs, waters uniform in
+    {1..serve_max_waters}, bases uniform over STO-3G / 6-31G* / cc-pVDZ, 10%
+    UHF doublets).  Sequential: one FP64 solve at a time.  Served: 8 slots,
+    mixed precision with FP64 refinement, all jobs submitted at once (an
+    arrival rate above capacity)."""
+    from hfgpu.serve import MIXED, build_inputs, make_stream, run_stream, summarize
+    jobs = make_stream(args.serve_jobs, rate=1000.0, max_waters=args.serve_max_waters, seed=4242)
+    inputs = build_inputs(jobs)
+    seq, span_seq = run_stream(jobs, slots=1, budget_bytes=120 << 30, honour_arrivals=False, inputs=inputs)
+    srv, span_srv = run_stream(jobs, slots=8, budget_bytes=120 << 30, honour_arrivals=False, inputs=inputs,
+                               jk=MIXED)
+    a, b = summarize(seq, span_seq), summarize(srv, span_srv)
+    de = max(abs(x["energy"] - y["energy"]) for x, y in zip(seq, srv) if x["status"] == 0 and y["status"] == 0)
+    return {"sample": "%d jobs, waters 1..%d, STO-3G/6-31G*/cc-pVDZ, 10%% UHF" % (len(jobs), args.serve_max_waters),
+            "sequential_fp64": a, "served_mixed_8_slots": b, "jobs_per_s_ratio": b["jobs_per_s"] / a["jobs_per_s"],
+            "max_abs_dE_served_vs_sequential": de}
+
+
+def measure_df(args, torch):
+    """DF J/K (hfg_df_jk) on (H2O)_n cc-pVDZ with def2-universal-JKFIT: build
+    time and J/K time per precision, and K-GEMM throughput (4 n^2 naux nocc
+    flops per build)."""
+    import time as _t
+    import numpy as np
+    from hfgpu import CartesianBasis, Context
+    from hfgpu.clusters import water_cluster
+    from hfgpu.lib import HFG_DF_BF16, HFG_DF_FP32, HFG_DF_FP64, DFTensor
+    atoms = water_cluster(args.df_waters)
+    ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
+    aux = CartesianBasis.build(atoms, "def2-universal-jkfit")
+    n, nocc = ctx.n, 5 * args.df_waters
+    q, _ = np.linalg.qr(np.random.default_rng(5).standard_normal((n, nocc)))
+    out = {"waters": args.df_waters, "n_ao": n, "naux": aux.n, "nocc": nocc}
+    ref = None
+    for name, storage in [("fp64", HFG_DF_FP64), ("tf32", HFG_DF_FP32), ("bf16", HFG_DF_BF16)]:
+        t0 = _t.time()
+        df = DFTensor(ctx, aux, pair_threshold=1e-12, storage=storage)
+        tb = _t.time() - t0
+        df.jk(q, mma=storage)
+        t0 = _t.time()
+        J, K = df.jk(q, mma=storage)
+        tj = _t.time() - t0
+        if ref is None:
+            ref = (J, K)
+        naux, rank, ncol = df.sizes()
+        out[name] = {"build_s": tb, "jk_s": tj, "rank": rank, "pairs": ncol,
+                     "k_gemm_tflops": 4.0 * n * n * rank * nocc / tj / 1e12,
+                     "max_abs_dJ_vs_fp64": float(np.max(np.abs(J - ref[0]))),
+                     "max_abs_dK_vs_fp64": float(np.max(np.abs(K - ref[1])))}
+        df.close()
+    return out
 
 
 def main():

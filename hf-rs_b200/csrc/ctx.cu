@@ -411,13 +411,76 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
   std::sort(plan->launches.begin(), plan->launches.end(), [](const Launch& x, const Launch& y) {
     return std::make_tuple(x.la + x.lb + x.lc + x.ld, x.fp32) > std::make_tuple(y.la + y.lb + y.lc + y.ld, y.fp32);
   });
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   for (auto& L : plan->launches) {
     L.st = ctx->stream;
+    // Work-queue steps.  Entries are ordered by the nominal cost of one of
+    // their warp tasks (bra x ket primitive pairs, before primitive
+    // screening), most expensive first, so that the cheap tasks form the
+    // tail of the launch; consecutive tasks are cut into steps of about equal
+    // nominal cost (about eight per resident warp, up to 32 warps per SM) and
+    // at most 64 tasks.  Each step's first task and its entry are tabulated,
+    // so no warp searches the prefix.
+    std::vector<double> cost;
+    {
+      const size_t ne = L.entries.size();
+      cost.resize(ne);
+      for (size_t e = 0; e < ne; ++e)
+        cost[e] = (double)ctx->h_pairs[L.entries[e].bra].npp * ctx->h_pairs[L.entries[e].k_lo].npp;
+      std::vector<size_t> ord(ne);
+      std::iota(ord.begin(), ord.end(), 0);
+      std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return cost[x] > cost[y]; });
+      std::vector<JKEntry> ents(ne);
+      std::vector<double> c2(ne);
+      L.prefix.assign(1, 0);
+      const int qpw = 32 / L.G;
+      for (size_t i = 0; i < ne; ++i) {
+        ents[i] = L.entries[ord[i]];
+        c2[i] = cost[ord[i]];
+        L.prefix.push_back(L.prefix.back() + (ents[i].k_hi - ents[i].k_lo + qpw - 1) / qpw);
+      }
+      L.entries.swap(ents);
+      cost.swap(c2);
+    }
+    const long long nw_total = L.prefix.back();
+    std::vector<long long> cstart;
+    std::vector<int> chunk_entry;
+    {
+      double total = 0.0;
+      for (size_t e = 0; e < L.entries.size(); ++e) total += cost[e] * (double)(L.prefix[e + 1] - L.prefix[e]);
+      const double target = total / ((double)sms * 32 * 8);
+      size_t e = 0;
+      long long t = 0;
+      while (t < nw_total) {
+        while (L.prefix[e + 1] <= t) ++e;
+        cstart.push_back(t);
+        chunk_entry.push_back((int)e);
+        double acc = 0.0;
+        long long k = 0;
+        size_t ee = e;
+        while (t < nw_total && k < 64 && (k == 0 || acc < target)) {
+          while (L.prefix[ee + 1] <= t) ++ee;
+          acc += cost[ee];
+          ++t;
+          ++k;
+        }
+      }
+      cstart.push_back(nw_total);
+      if (chunk_entry.empty()) chunk_entry.push_back(0);
+    }
+    L.nchunks = (long long)cstart.size() - 1;
     HFG_CUDA(ctx, cudaMallocAsync((void**)&L.d_entries, L.entries.size() * sizeof(JKEntry), ctx->stream));
     HFG_CUDA(ctx, cudaMallocAsync((void**)&L.d_prefix, L.prefix.size() * sizeof(long long), ctx->stream));
+    HFG_CUDA(ctx, cudaMallocAsync((void**)&L.d_cstart, cstart.size() * sizeof(long long), ctx->stream));
+    HFG_CUDA(ctx, cudaMemcpyAsync(L.d_cstart, cstart.data(), cstart.size() * sizeof(long long),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    HFG_CUDA(ctx, cudaMallocAsync((void**)&L.d_chunk, chunk_entry.size() * sizeof(int), ctx->stream));
     HFG_CUDA(ctx, cudaMemcpyAsync(L.d_entries, L.entries.data(), L.entries.size() * sizeof(JKEntry),
                                   cudaMemcpyHostToDevice, ctx->stream));
     HFG_CUDA(ctx, cudaMemcpyAsync(L.d_prefix, L.prefix.data(), L.prefix.size() * sizeof(long long),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    HFG_CUDA(ctx, cudaMemcpyAsync(L.d_chunk, chunk_entry.data(), chunk_entry.size() * sizeof(int),
                                   cudaMemcpyHostToDevice, ctx->stream));
     HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     // the host copies are no longer needed beyond the counts
@@ -524,6 +587,9 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
     a.counter = ctx->d_counters.p + l;
     a.entries = L.d_entries;
     a.prefix = L.d_prefix;
+    a.chunk_entry = L.d_chunk;
+    a.chunk_start = L.d_cstart;
+    a.nchunks = L.nchunks;
     a.nentries = (int)L.prefix[0];
     a.nwarps = L.prefix[1];
     HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.G, L.fp32, a, ctx->stream));
@@ -562,6 +628,8 @@ hfg_ctx::~hfg_ctx() {
     for (auto& L : kv.second->launches) {
       if (L.d_entries) cudaFreeAsync(L.d_entries, L.st);
       if (L.d_prefix) cudaFreeAsync(L.d_prefix, L.st);
+      if (L.d_chunk) cudaFreeAsync(L.d_chunk, L.st);
+      if (L.d_cstart) cudaFreeAsync(L.d_cstart, L.st);
     }
   d_pairs.release();
   d_prims.release();
@@ -756,6 +824,54 @@ int hfg_jk(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* Pt, c
   if (rc != HFG_OK) return rc;
   HFG_CUDA(ctx, cudaMemcpyAsync(J, ctx->d_J.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
   HFG_CUDA(ctx, cudaMemcpyAsync(K, ctx->d_K.p, nspin * nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return HFG_OK;
+}
+
+// Packed tensor on the device: every quartet of the FP64 plan without
+// primitive screening (the plan holds each unique significant shell quartet
+// once), stored by eri_packed_kernel.
+static int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len) {
+  const size_t n = (size_t)ctx->n, np = n * (n + 1) / 2;
+  if (len != np * (np + 1) / 2)
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "packed length must be n_p (n_p + 1) / 2 with n_p = n (n + 1) / 2");
+  if (!(thr >= 0.0)) return set_error(ctx, HFG_ERR_INVALID_INPUT, "Schwarz threshold must be >= 0");
+  Plan* plan = nullptr;
+  int rc = build_plan(ctx, thr, 0.0, 0.0, HFG_FP64, plan);
+  if (rc != HFG_OK) return rc;
+  HFG_CUDA(ctx, cudaMemsetAsync(d_out, 0, len * sizeof(double), ctx->stream));
+  for (const Launch& L : plan->launches) {
+    if (L.G != 1) return set_error(ctx, HFG_ERR_UNSUPPORTED, "packed tensor: cooperative launch groups");
+    HFG_CUDA(ctx, launch_eri_packed(L.la, L.lb, L.lc, L.ld, L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1],
+                                    ctx->d_pairs.p, ctx->d_rec64.p, ctx->d_boys64.p, ctx->d_expt64.p, d_out,
+                                    ctx->stream));
+  }
+  return HFG_OK;
+}
+
+int hfg_eri_packed_device(hfg_ctx* ctx, double schwarz_threshold, double* d_out, size_t len) {
+  if (!ctx) return HFG_ERR_INVALID_INPUT;
+  if (!d_out) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  AllocScope alloc_scope(ctx->stream);
+  cudaSetDevice(ctx->device);
+  return eri_packed_locked(ctx, schwarz_threshold, d_out, len);
+}
+
+int hfg_eri_packed(hfg_ctx* ctx, double schwarz_threshold, double* out, size_t len) {
+  if (!ctx) return HFG_ERR_INVALID_INPUT;
+  if (!out) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  AllocScope alloc_scope(ctx->stream);
+  cudaSetDevice(ctx->device);
+  DevBuf<double> buf;
+  if (buf.alloc(len) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(ctx, HFG_ERR_OOM, "packed tensor does not fit in device memory");
+  }
+  int rc = eri_packed_locked(ctx, schwarz_threshold, buf.p, len);
+  if (rc != HFG_OK) return rc;
+  HFG_CUDA(ctx, cudaMemcpyAsync(out, buf.p, len * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return HFG_OK;
 }

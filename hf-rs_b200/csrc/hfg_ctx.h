@@ -35,6 +35,9 @@ struct Launch {
   std::vector<long long> prefix;
   JKEntry* d_entries = nullptr;
   long long* d_prefix = nullptr;
+  int* d_chunk = nullptr;             // entry of the first task of every work-queue step
+  long long* d_cstart = nullptr;      // first task of every step (nchunks + 1)
+  long long nchunks = 0;
 };
 
 struct Plan {

@@ -47,8 +47,11 @@ struct JKEntry {
 
 struct JKLaunchArgs {
   const JKEntry* entries;
-  const long long* prefix;  // warp-chunk prefix over entries (size nentries + 1)
+  const long long* prefix;  // warp-task prefix over entries (size nentries + 1)
+  const long long* chunk_start;  // work-queue steps: tasks [chunk_start[c], chunk_start[c + 1])
+  const int* chunk_entry;        // entry holding the first task of each step
   int nentries;
+  long long nchunks;
   long long nwarps;
   const PairInfo* pairs;
   const PrimRec64* rec64;

@@ -27,7 +27,7 @@ static cudaError_t launch_t(const JKLaunchArgs& a, cudaStream_t st) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem);
     return sms * (per_sm > 0 ? per_sm : 1);
   }();
-  const long long want = (a.nwarps + kChunk * (block / 32) - 1) / (kChunk * (block / 32));
+  const long long want = (a.nchunks + (block / 32) - 1) / (block / 32);
   const long long grid = want < resident ? want : resident;
   if (grid <= 0) return cudaSuccess;
   kern<<<(unsigned)grid, block, smem, st>>>(a);

@@ -1,6 +1,6 @@
 // Dispatch tables for the J/K, Schwarz and single-quartet kernels.
 #include "jk_dispatch.h"
-#include "jk_kernels.cuh"
+#include "eri_prim.cuh"
 
 namespace hfg {
 

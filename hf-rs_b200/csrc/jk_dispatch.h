@@ -62,6 +62,9 @@ cudaError_t launch_count(const JKEntry* entries, const long long* prefix, int ne
                          const PairInfo* pairs, const float* pbound, double eps, unsigned long long* out,
                          cudaStream_t st);
 cudaError_t fma_peak(int fp32, double* tflops);
+cudaError_t launch_eri_packed(int la, int lb, int lc, int ld, const JKEntry* entries, const long long* prefix,
+                              int nentries, long long nwarps, const PairInfo* pairs, const PrimRec64* rec,
+                              const double* boys, const double* expt, double* out, cudaStream_t st);
 cudaError_t launch_quartet(int la, int lb, int lc, int ld, const PairInfo* pairs, const PrimPair* prims,
                            const double* boys, const double* expt, double* out, cudaStream_t st);
 

@@ -119,6 +119,9 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
     a.counter = counters + l;
     a.entries = L.d_entries;
     a.prefix = L.d_prefix;
+    a.chunk_entry = L.d_chunk;
+    a.chunk_start = L.d_cstart;
+    a.nchunks = L.nchunks;
     a.nentries = (int)L.prefix[0];
     a.nwarps = L.prefix[1];
     rc = hfg::cuda_check(ctx, hfg::launch_jk(L.la, L.lb, L.lc, L.ld, L.G, L.fp32, a, ctx->stream), "J/K launch");

@@ -596,6 +596,8 @@ void hfg_scf_opts_default(hfg_scf_opts* o) {
   hfg_jk_opts_default(&o->jk);
   o->refine_iters = 2;
   o->diis_size = 8;
+  o->incremental_tol = 1e-12;
+  o->rebuild_every = 8;
 }
 
 int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_out, double* F_out, double* C_out,
@@ -748,6 +750,64 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   hfg_jk_opts jo = o->jk;
   hfg_jk_opts jo64 = o->jk;
   jo64.precision = HFG_FP64;
+  // Incremental builds in the mixed phase: J/K are linear in the density, so
+  // J(P) = J(P_full) + J(P - P_full) summed over the builds since the last
+  // full one, and the change only needs the quartets with
+  // Q_ab Q_cd max|dP| >= incremental_tol (a Schwarz threshold scaled by
+  // 1 / max|dP|, rounded down to a decade so that few plans are built).
+  // The FP64 refinement and the final Fock matrices are full builds.
+  const bool incremental = mixed && o->incremental_tol > 0.0;
+  const int rebuild_every = std::max(1, o->rebuild_every);
+  DevBuf<double> Jinc, Kinc, Pinc, dP;
+  if (incremental) {
+    CK(Jinc.alloc(nn));
+    CK(Kinc.alloc(nspin * nn));
+    CK(Pinc.alloc(nspin * nn));
+    CK(dP.alloc((nspin + 1) * nn));
+  }
+  int since_full = -1, builds_inc = 0;
+  auto fock_mixed = [&]() -> int {
+    if (!incremental) return fock(jo);
+    if (since_full < 0 || since_full >= rebuild_every) {
+      RK(fock(jo));
+      CK(cudaMemcpyAsync(Jinc.p, J.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(Kinc.p, K.p, nspin * nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(Pinc.p, P.p, nspin * nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+      since_full = 0;
+      return HFG_OK;
+    }
+    double dmax = 0.0;
+    for (int sp = 0; sp < nspin; ++sp) {
+      CK(cudaMemcpyAsync(dP.p + sp * nn, P.p + sp * nn, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+      axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(dP.p + sp * nn, Pinc.p + sp * nn, -1.0, 1.0, nn);
+      dmax = std::max(dmax, s.maxabs(dP.p + sp * nn, nn));
+    }
+    const double* dpt = dP.p;
+    if (uhf) {
+      CK(cudaMemcpyAsync(dP.p + 2 * nn, dP.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+      axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(dP.p + 2 * nn, dP.p + nn, 1.0, 1.0, nn);
+      dpt = dP.p + 2 * nn;
+    }
+    if (dmax > 0.0) {
+      hfg_jk_opts ji = jo;
+      double thr = std::max(o->incremental_tol / dmax, jo.schwarz_threshold);
+      ji.schwarz_threshold = std::pow(10.0, std::floor(std::log10(thr) + 1e-9));
+      RK(jk_device_locked(ctx, &ji, nspin, dpt, dP.p, J.p, K.p));
+      ++buildsmix;
+      ++builds_inc;
+      axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(Jinc.p, J.p, 1.0, 1.0, nn);
+      axpby_kernel<<<nblk(nspin * nn), 256, 0, ctx->stream>>>(Kinc.p, K.p, 1.0, 1.0, nspin * nn);
+      CK(cudaMemcpyAsync(Pinc.p, P.p, nspin * nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    ++since_full;
+    for (int sp = 0; sp < nspin; ++sp) {
+      double* f = F.p + sp * nn;
+      CK(cudaMemcpyAsync(f, s.H.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+      axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(f, Jinc.p, 1.0, 1.0, nn);
+      axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(f, Kinc.p + sp * nn, uhf ? -1.0 : -0.5, 1.0, nn);
+    }
+    return HFG_OK;
+  };
   bool refining = !mixed;
   int refine_done = 0;
   double prev_e = 0.0, e_tot = 0.0;
@@ -757,7 +817,8 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   std::vector<int> slot;   // history slot of each stored vector, oldest first
   CK(cudaMemcpyAsync(Pprev.p, P.p, nspin * nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
   for (it = 1; it <= o->max_iter; ++it) {
-    RK(fock(refining ? jo64 : jo));
+    if (refining) RK(fock(jo64));
+    else RK(fock_mixed());
     if (refining) ++refine_done;
     e_tot = energy() + e_nuc;
     const double de = std::fabs(e_tot - prev_e);
@@ -880,6 +941,7 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   res->n_mo = m;
   res->fock_builds_fp64 = builds64;
   res->fock_builds_mixed = buildsmix;
+  res->fock_builds_incremental = builds_inc;
   if (uhf) {
     // <S^2> = S(S+1) + N_b - sum |(C_a^T S C_b)_ij|^2 over occupied
     RK(s.gemm(CUBLAS_OP_N, CUBLAS_OP_N, n, nb > 0 ? nb : 1, n, 1.0, s.S.p, n, C.p + (long long)n * m, n, 0.0, s.tmp1.p, n));

@@ -30,14 +30,16 @@ __global__ void count_kernel(const JKEntry* __restrict__ entries, const long lon
     const PairInfo b = pairs[e.bra], q = pairs[k];
     // the kernels' loop: ket primitive pairs surviving against the largest bra
     // one, then bra primitive pairs while the product stays above eps
-    const double bmax = pbound[b.pp_off];
+    // (FP32 products, as in the kernels)
+    const float feps = (float)eps;
+    const float bmax = pbound[b.pp_off];
     for (int ik = 0; ik < q.npp; ++ik) {
-      const double qb = pbound[q.pp_off + ik];
-      if (qb * bmax < eps) break;
+      const float qb = pbound[q.pp_off + ik];
+      if (qb * bmax < feps) break;
       int l = 0, h = b.npp;  // bounds sorted descending
       while (l < h) {
         const int m = (l + h) >> 1;
-        if ((double)pbound[b.pp_off + m] * qb >= eps) l = m + 1; else h = m;
+        if (pbound[b.pp_off + m] * qb >= feps) l = m + 1; else h = m;
       }
       c += (unsigned long long)l;
     }

@@ -12,7 +12,9 @@ STATUS = {0: "OK", 1: "INVALID_INPUT", 2: "INTEGRAL", 3: "SCF", 4: "OOM", 5: "TI
 
 
 def library_path():
-    return os.path.join(PKG_ROOT, "libhfg.so")
+    """The in-tree libhfg.so, or the build named by HFG_LIBRARY (a tuning
+    build of the same sources)."""
+    return os.environ.get("HFG_LIBRARY") or os.path.join(PKG_ROOT, "libhfg.so")
 
 
 class HfgError(RuntimeError):
@@ -48,14 +50,16 @@ class SCFOptions(ctypes.Structure):
                 ("multiplicity", ctypes.c_int), ("uhf", ctypes.c_int), ("spherical", ctypes.c_int),
                 ("max_iter", ctypes.c_int), ("energy_tol", ctypes.c_double), ("residual_tol", ctypes.c_double),
                 ("density_tol", ctypes.c_double), ("jk", JKOptions), ("refine_iters", ctypes.c_int),
-                ("diis_size", ctypes.c_int), ("verbose", ctypes.c_int), ("guess", ctypes.c_int)]
+                ("diis_size", ctypes.c_int), ("verbose", ctypes.c_int), ("guess", ctypes.c_int),
+                ("incremental_tol", ctypes.c_double), ("rebuild_every", ctypes.c_int)]
 
 
 class SCFResult(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("electronic", ctypes.c_double), ("nuclear", ctypes.c_double),
                 ("energy_before_refinement", ctypes.c_double), ("s2", ctypes.c_double),
                 ("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("n_mo", ctypes.c_int),
-                ("fock_builds_fp64", ctypes.c_int), ("fock_builds_mixed", ctypes.c_int), ("time_ms", ctypes.c_double)]
+                ("fock_builds_fp64", ctypes.c_int), ("fock_builds_mixed", ctypes.c_int), ("time_ms", ctypes.c_double),
+                ("fock_builds_incremental", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -127,6 +131,8 @@ def load_library():
     L.hfg_ctx_sizes.argtypes = [VP, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_long)]
     L.hfg_schwarz.argtypes = [VP, DP, ctypes.c_long]
     L.hfg_shell_quartet.argtypes = [VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP]
+    L.hfg_eri_packed.argtypes = [VP, ctypes.c_double, DP, ctypes.c_size_t]
+    L.hfg_eri_packed_device.argtypes = [VP, ctypes.c_double, VP, ctypes.c_size_t]
     L.hfg_jk.argtypes = [VP, P(JKOptions), ctypes.c_int, DP, DP, DP, DP]
     L.hfg_jk_device.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
     L.hfg_jk_device_noalloc.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
@@ -219,6 +225,16 @@ class Context:
         self._check(self.lib.hfg_shell_quartet(self.h, a, b, c, d, _dp(out)))
         return out
 
+    def eri_packed(self, threshold=1e-12, length=None):
+        """Packed 8-fold ERI tensor (hfg_eri_packed), hf-rs's compute_eri_tensor
+        layout."""
+        n = self.n
+        npair = n * (n + 1) // 2
+        length = npair * (npair + 1) // 2 if length is None else length
+        out = np.zeros(length)
+        self._check(self.lib.hfg_eri_packed(self.h, threshold, _dp(out), length))
+        return out
+
     def jk(self, P_total, P_spin=None, opts=None):
         """J and K (list) from host densities (hfg_jk)."""
         n = self.n
@@ -254,8 +270,10 @@ class Context:
         return Fa, Fb
 
     def scf(self, charge=0, multiplicity=1, uhf=False, spherical=False, tol=1e-10, max_iter=100, jk=None,
-            refine_iters=2, verbose=False, want=("P", "F"), guess="sad"):
-        """Device SCF (hfg_scf) for the context's molecule; returns a dict."""
+            refine_iters=2, verbose=False, want=("P", "F"), guess="sad", incremental=1e-12, rebuild_every=8):
+        """Device SCF (hfg_scf) for the context's molecule; returns a dict.
+        `incremental` (mixed J/K only): screening tolerance of the builds from
+        density changes, 0 for a full build every iteration."""
         b = self.basis
         o = SCFOptions()
         self.lib.hfg_scf_opts_default(ctypes.byref(o))
@@ -271,6 +289,8 @@ class Context:
         o.refine_iters = refine_iters
         o.verbose = int(verbose)
         o.guess = 0 if guess == "sad" else 1
+        o.incremental_tol = incremental
+        o.rebuild_every = rebuild_every
         n = self.n
         ns = 2 if uhf else 1
         P = np.zeros((ns, n, n)) if "P" in want else None

@@ -92,6 +92,19 @@ int hfg_schwarz(hfg_ctx* ctx, double* bounds, long n);
 int hfg_shell_quartet(hfg_ctx* ctx, int a, int b, int c, int d, double* out);
 
 /*
+ * compute_eri_tensor (src/scf.rs:275-333, built by compute_shell_eri_tensor,
+ * src/shell_integrals.rs:156-240): the packed 8-fold tensor of Cartesian
+ * integrals, slot c(c(mu,nu), c(lam,sig)) with c(i,j) = i(i+1)/2 + j for
+ * i >= j (src/scf.rs:222-235); shell quartets with Q_ab Q_cd <= threshold
+ * stay zero (hf-rs uses 1e-12).  len must be n_p (n_p + 1) / 2 with
+ * n_p = n (n + 1) / 2.  hfg_eri_packed fills a host array (the tensor is
+ * built on the device, which needs len doubles of device memory);
+ * hfg_eri_packed_device fills a device array on the context stream.
+ */
+int hfg_eri_packed(hfg_ctx* ctx, double schwarz_threshold, double* out, size_t len);
+int hfg_eri_packed_device(hfg_ctx* ctx, double schwarz_threshold, double* d_out, size_t len);
+
+/*
  * Stands in for compute_eri_tensor (src/scf.rs:275) followed by
  * contract_jk (src/scf.rs:337-364), without storing the integrals: a direct
  * J/K build from densities.  P_total (n x n) gives J; P_spin holds nspin
@@ -189,6 +202,10 @@ typedef struct {
   int verbose;             /* iteration table on stderr */
   int guess;               /* 0: superposition of atomic densities (hf-rs's default, src/sad.rs),
                               1: core Hamiltonian */
+  double incremental_tol;  /* HFG_MIXED phase only: J/K built from the density change dP since the
+                              last full build, skipping shell quartets with Q_ab Q_cd max|dP| below
+                              this (1e-12 by default; 0: a full build every iteration) */
+  int rebuild_every;       /* full build after this many incremental ones (default 8) */
 } hfg_scf_opts;
 
 typedef struct {
@@ -198,11 +215,13 @@ typedef struct {
   int iterations, converged, n_mo;
   int fock_builds_fp64, fock_builds_mixed;
   double time_ms;
+  int fock_builds_incremental;     /* of the mixed builds, those from a density change */
 } hfg_scf_result;
 
 /* Defaults: RHF singlet, 100 iterations, tolerances derived from 1e-10 as
    run_scf_in_space does (src/scf.rs:393-399), FP64 J/K, 2 refinement
-   iterations, CDIIS(8). */
+   iterations, CDIIS(8), incremental mixed builds at 1e-12 with a full
+   build every 8. */
 void hfg_scf_opts_default(hfg_scf_opts* opts);
 
 /*

@@ -73,13 +73,28 @@ def test_water_cluster_rhf_vs_oracle(nw):
     assert abs(r["energy"] - ref["energy"]) <= 1e-10
 
 
-def test_mixed_precision_scf_refines_to_fp64():
+@pytest.mark.parametrize("incremental", [0.0, 1e-12])
+def test_mixed_precision_scf_refines_to_fp64(incremental):
+    # mixed phase (full or incremental builds) then FP64 refinement: the
+    # energy of the plain FP64 SCF within 1e-8 Eh
     atoms = water_cluster(4)
     ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
     e64 = ctx.scf(spherical=True, tol=1e-10)["energy"]
-    r = ctx.scf(spherical=True, tol=1e-10, jk=JKOptions.make(prim=1e-15, mixed=1e-7))
+    r = ctx.scf(spherical=True, tol=1e-10, jk=JKOptions.make(prim=1e-15, mixed=1e-7), incremental=incremental)
     assert r["converged"] and r["fock_builds_mixed"] > 0 and r["fock_builds_fp64"] >= 2
+    assert (r["fock_builds_incremental"] > 0) == (incremental > 0)
     assert abs(r["energy"] - e64) <= 1e-8
+
+
+def test_mixed_incremental_uhf_doublet():
+    atoms = water_cluster(2)
+    ctx = Context(CartesianBasis.build(atoms, "6-31g*"))
+    e64 = ctx.scf(charge=1, multiplicity=2, uhf=True, tol=1e-10, max_iter=200)
+    r = ctx.scf(charge=1, multiplicity=2, uhf=True, tol=1e-10, max_iter=200,
+                jk=JKOptions.make(prim=1e-15, mixed=1e-7))
+    assert e64["converged"] and r["converged"] and r["fock_builds_incremental"] > 0
+    assert abs(r["energy"] - e64["energy"]) <= 1e-8
+    assert abs(r["s2"] - e64["s2"]) < 1e-6
 
 
 def test_uhf_doublet_cation_vs_oracle():
