@@ -36,7 +36,7 @@ def workload(waters, n_ao):
     return "(H2O)%d cc-pVDZ direct RHF Fock build (J+K), %d Cartesian AOs, Schwarz 1e-12" % (waters, n_ao)
 SCHWARZ = 1e-12
 PRIM = 1e-15
-MIXED = 1e-7
+TUNE_BUDGET = 5e-9
 
 
 def parse():
@@ -270,9 +270,10 @@ def run_ours(args):
     basis = CartesianBasis.build(atoms, "cc-pvdz")
     n = basis.n
     ctx = Context(basis, device=local, stream=stream.cuda_stream)
-    rng = np.random.default_rng(11)
-    Ph = rng.standard_normal((n, n)) * 0.1
-    Ph = Ph + Ph.T
+    # a physical density: three SCF iterations from the SAD guess (FP64 J/K)
+    scf = ctx.scf(spherical=True, tol=1e-10, max_iter=3, jk=JKOptions.make(schwarz=SCHWARZ, prim=1e-15),
+                  want=("P",))
+    Ph = np.ascontiguousarray(scf["P"][0])
     P = torch.from_numpy(Ph).to(dev)
     J = torch.empty((n, n), dtype=torch.float64, device=dev)
     K = torch.empty((n, n), dtype=torch.float64, device=dev)
@@ -281,31 +282,39 @@ def run_ours(args):
     def flush():
         flush_buf.zero_()
 
-    opt_mixed = JKOptions.make(schwarz=SCHWARZ, prim=PRIM, mixed=MIXED)
-    opt_fp64 = JKOptions.make(schwarz=SCHWARZ, prim=PRIM)
-
-    def build(opt):
-        return lambda: ctx.jk_device(P.data_ptr(), P.data_ptr(), J.data_ptr(), K.data_ptr(), 1, opt)
-
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    torch.cuda.synchronize()
+    # mixed form chosen by the autotuner (FP32 threshold 1e-9..1e-6, primitive
+    # threshold 1e-15..1e-13, build energy error within 5e-9 Eh of the plain
+    # FP64 build); untimed
+    opt_mixed, tune = ctx.autotune(P.data_ptr(), P.data_ptr(), base=JKOptions.make(schwarz=SCHWARZ),
+                                   max_energy_error=TUNE_BUDGET, repeats=1)
+    opt_plain = JKOptions.make(schwarz=SCHWARZ)            # the reference's arithmetic in FP64
+    opt_fp64 = JKOptions.make(schwarz=SCHWARZ, prim=PRIM)  # FP64 with primitive screening
+
+    def build(opt):
+        return lambda: ctx.jk_device(P.data_ptr(), P.data_ptr(), J.data_ptr(), K.data_ptr(), 1, opt)
+
     # warm-up (plans are built on first use)
     for _ in range(args.warmup):
         build(opt_mixed)()
-        build(opt_fp64)()
+    build(opt_fp64)()
     torch.cuda.synchronize()
-    stats_mixed = None
     build(opt_mixed)()
     stats_mixed = ctx.last_stats()
     Jm, Km = J.cpu().numpy().copy(), K.cpu().numpy().copy()
     build(opt_fp64)()
     stats_fp64 = ctx.last_stats()
+    build(opt_plain)()
+    stats_plain = ctx.last_stats()
     Jf, Kf = J.cpu().numpy().copy(), K.cpu().numpy().copy()
     jk_diff = float(max(np.max(np.abs(Jm - Jf)), np.max(np.abs(Km - Kf))))
+    dE_build = float(0.5 * np.sum(Ph * (Jm - Jf)) - 0.25 * np.sum(Ph * (Km - Kf)))
 
     clocks = Clocks(local)
     barrier()
@@ -313,6 +322,8 @@ def run_ours(args):
     t_mixed = timed(torch, stream, build(opt_mixed), args.steps, flush)
     barrier()
     t_fp64 = timed(torch, stream, build(opt_fp64), args.steps, flush)
+    barrier()
+    t_plain = timed(torch, stream, build(opt_plain), args.steps, flush)
     barrier()
     ck = clocks.stop()
 
@@ -325,8 +336,10 @@ def run_ours(args):
 
     tot_mixed = max_over_ranks(sum(t_mixed))
     tot_fp64 = max_over_ranks(sum(t_fp64))
+    tot_plain = max_over_ranks(sum(t_plain))
     value = world * args.steps / (tot_mixed / 1000.0)
     value_fp64 = world * args.steps / (tot_fp64 / 1000.0)
+    value_plain = world * args.steps / (tot_plain / 1000.0)
 
     e2e = None
     if not args.no_e2e:
@@ -390,21 +403,30 @@ def run_ours(args):
     dfres = None
     if world == 1 and args.df_waters > 0:
         dfres = measure_df(args, torch)
+    mt, pt = opt_mixed.mixed_threshold, opt_mixed.prim_threshold
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_mixed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32-mixed", "data": "synthetic",
-            "config": {"workload": workload(args.waters, n) + ", mixed precision (FP32 below Q_ab*Q_cd < %g), primitive "
-                                              "screening %g" % (MIXED, PRIM),
+            "config": {"workload": workload(args.waters, n) + ", mixed precision (FP32 below Q_ab*Q_cd < %g, "
+                                   "primitive screening %g; autotuned)" % (mt, pt),
                        "n_ao": n, "waters": args.waters, "parallelism": "replicas" if world > 1 else "single",
+                       "density": "SCF density after 3 iterations from the SAD guess",
                        "l2": "flushed (256 MB write) before every timed step"},
+            "mixed_energy_error_per_build": dE_build,
+            "jk_max_abs_diff_mixed_vs_plain_fp64": jk_diff,
+            "fp64_plain": {"value": value_plain, "unit": UNIT, "ms_per_step": tot_plain / args.steps,
+                           "form": "FP64, Schwarz screening only (the reference's arithmetic)",
+                           "wmd_flops": stats_plain["wmd_flops_fp64"]},
             "fp64": {"value": value_fp64, "unit": UNIT, "ms_per_step": tot_fp64 / args.steps,
-                     "wmd_flops": stats_fp64["wmd_flops_fp64"]},
-            "mixed_over_fp64": value / value_fp64, "jk_max_abs_diff_mixed_vs_fp64": jk_diff,
+                     "form": "FP64 with primitive screening %g" % PRIM, "wmd_flops": stats_fp64["wmd_flops_fp64"]},
+            "mixed_over_fp64_plain": value / value_plain, "mixed_over_fp64": value / value_fp64,
+            "autotune": {"chosen": {"fp32_threshold": mt, "prim_threshold": pt}, "budget_eh": TUNE_BUDGET,
+                         "candidates": tune["candidates"]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck, "serving": serving, "df": dfres,
             # per build: the plan's J/K launches plus two symmetrisation kernels;
-            # timed: K mixed builds, K FP64 builds and K end-to-end mixed builds
+            # timed: K mixed, K FP64, K plain FP64 and K end-to-end mixed builds
             "gpu_launches": args.steps * (stats_mixed["launches"] + 2) * (1 if e2e is None else 2)
-            + args.steps * (stats_fp64["launches"] + 2)}
+            + args.steps * (stats_fp64["launches"] + 2) + args.steps * (stats_plain["launches"] + 2)}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

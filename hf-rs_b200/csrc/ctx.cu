@@ -290,23 +290,37 @@ static int build_pairs(hfg_ctx* ctx) {
                                 cudaMemcpyHostToDevice, ctx->stream));
   HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_prims.p, ctx->h_prims.data(), ctx->h_prims.size() * sizeof(PrimPair),
                                 cudaMemcpyHostToDevice, ctx->stream));
-  // compact records for the J/K kernels
+  // compact records for the J/K kernels, interleaved within each pair class:
+  // record k of the class's pair p at base + k * count + p (all pairs of a
+  // class have the same primitive count)
   const size_t npp = ctx->h_prims.size();
   std::vector<PrimRec64> r64(npp);
   std::vector<PrimRec32> r32(npp);
   std::vector<float> pb(npp);
-  for (const auto& pi : ctx->h_pairs) {
-    const double ab2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
-    for (int k = 0; k < pi.npp; ++k) {
-      const PrimPair& q = ctx->h_prims[pi.pp_off + k];
-      // P - A = -(beta/p) AB; recover beta/p from the stored P - A
-      double bp = 0.0;
-      if (ab2 > 0.0) bp = -(q.PAx * pi.ABx + q.PAy * pi.ABy + q.PAz * pi.ABz) / ab2;
-      r64[pi.pp_off + k] = {q.p, q.inv_p, q.kp, bp};
-      r32[pi.pp_off + k] = {(float)q.p, (float)q.inv_p, (float)q.kp, (float)bp};
-      pb[pi.pp_off + k] = (float)q.bound;
+  {
+    size_t base = 0;
+    for (const auto& c : ctx->classes) {
+      for (int p = 0; p < c.count; ++p) {
+        PairInfo& pi = ctx->h_pairs[c.first + p];
+        pi.rec_off = (int)(base + p);
+        pi.rec_stride = c.count;
+        const double ab2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
+        for (int k = 0; k < pi.npp; ++k) {
+          const PrimPair& q = ctx->h_prims[pi.pp_off + k];
+          // P - A = -(beta/p) AB; recover beta/p from the stored P - A
+          double bp = 0.0;
+          if (ab2 > 0.0) bp = -(q.PAx * pi.ABx + q.PAy * pi.ABy + q.PAz * pi.ABz) / ab2;
+          const size_t r = base + (size_t)k * c.count + p;
+          r64[r] = {q.p, q.inv_p, q.kp, bp};
+          r32[r] = {(float)q.p, (float)q.inv_p, (float)q.kp, (float)bp};
+          pb[r] = (float)q.bound;
+        }
+      }
+      base += (size_t)c.count * (size_t)c.Ka * c.Kb;
     }
   }
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_pairs.p, ctx->h_pairs.data(), ctx->h_pairs.size() * sizeof(PairInfo),
+                                cudaMemcpyHostToDevice, ctx->stream));
   HFG_CUDA(ctx, ctx->d_rec64.alloc(npp));
   HFG_CUDA(ctx, ctx->d_rec32.alloc(npp));
   HFG_CUDA(ctx, ctx->d_pbound.alloc(npp));
@@ -533,6 +547,31 @@ __global__ void symmetrize_kernel(const double* __restrict__ acc, double* __rest
   const int i = (int)(r / n), j = (int)(r % n);
   out[t] = 0.5 * (acc[m * nn + (long long)i * n + j] + acc[m * nn + (long long)j * n + i]);
 }
+
+// a -= b
+__global__ void axpy_sub_kernel(double* __restrict__ a, const double* __restrict__ b, long long len) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < len) a[t] -= b[t];
+}
+
+// out += w * sum a[i] b[i] (one atomic per block of 256 threads)
+__global__ void wdot_kernel(const double* __restrict__ a, const double* __restrict__ b, long long len, double w,
+                            double* __restrict__ out) {
+  double s = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    s += a[i] * b[i];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  __shared__ double part[8];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += part[k];
+    atomicAdd(out, t * w);
+  }
+}
+
+static unsigned nblk(long long len) { return (unsigned)((len + 255) / 256); }
 
 __global__ void fock_kernel(const double* __restrict__ H, const double* __restrict__ J, const double* __restrict__ K,
                             double* __restrict__ F, double kscale, long long nn) {
@@ -924,6 +963,125 @@ int hfg_fock_rhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const d
 int hfg_fock_uhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* Pa, const double* Pb,
                  double* Fa, double* Fb) {
   return fock_common(ctx, opts, H, Pa, Pb, Fa, Fb, 1);
+}
+
+void hfg_autotune_opts_default(hfg_autotune_opts* o) {
+  *o = hfg_autotune_opts{};
+  const double f[4] = {1e-9, 1e-8, 1e-7, 1e-6}, p[3] = {1e-15, 1e-14, 1e-13};
+  for (int i = 0; i < 4; ++i) o->fp32_thresholds[i] = f[i];
+  o->n_fp32 = 4;
+  for (int i = 0; i < 3; ++i) o->prim_thresholds[i] = p[i];
+  o->n_prim = 3;
+  o->max_energy_error = 5e-9;
+  o->repeats = 2;
+}
+
+int hfg_jk_autotune(hfg_ctx* ctx, const hfg_jk_opts* base, int nspin, const double* dPt, const double* dPs,
+                    const hfg_autotune_opts* opts, hfg_autotune_result* res) {
+  if (!ctx) return HFG_ERR_INVALID_INPUT;
+  if (!dPt || !dPs || !res) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  if (nspin < 1 || nspin > 2) return set_error(ctx, HFG_ERR_INVALID_INPUT, "nspin must be 1 or 2");
+  hfg_autotune_opts o;
+  hfg_autotune_opts_default(&o);
+  if (opts) {
+    if (opts->n_fp32 < 0 || opts->n_fp32 > 8 || opts->n_prim < 0 || opts->n_prim > 8)
+      return set_error(ctx, HFG_ERR_INVALID_INPUT, "at most 8 candidates per list");
+    if (opts->n_fp32 > 0) {
+      o.n_fp32 = opts->n_fp32;
+      for (int i = 0; i < o.n_fp32; ++i) o.fp32_thresholds[i] = opts->fp32_thresholds[i];
+    }
+    if (opts->n_prim > 0) {
+      o.n_prim = opts->n_prim;
+      for (int i = 0; i < o.n_prim; ++i) o.prim_thresholds[i] = opts->prim_thresholds[i];
+    }
+    if (opts->max_energy_error > 0.0) o.max_energy_error = opts->max_energy_error;
+    if (opts->repeats > 0) o.repeats = opts->repeats;
+  }
+  hfg_jk_opts b;
+  if (base) b = *base; else hfg_jk_opts_default(&b);
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  AllocScope alloc_scope(ctx->stream);
+  cudaSetDevice(ctx->device);
+  const long long nn = (long long)ctx->n * ctx->n;
+  DevBuf<double> J64, K64, J, K, e;
+  HFG_CUDA(ctx, J64.alloc(nn));
+  HFG_CUDA(ctx, K64.alloc(nspin * nn));
+  HFG_CUDA(ctx, J.alloc(nn));
+  HFG_CUDA(ctx, K.alloc(nspin * nn));
+  HFG_CUDA(ctx, e.alloc(1));
+  struct Events {
+    cudaEvent_t a = nullptr, b = nullptr;
+    Events() {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+    }
+    ~Events() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } ev;
+  // a build with options jo into (dJ, dK): one untimed build (it makes the
+  // plan), then the minimum device time over `reps` builds
+  auto run = [&](const hfg_jk_opts& jo, double* dJ, double* dK, int reps, double& ms) -> int {
+    int rc = jk_device_locked(ctx, &jo, nspin, dPt, dPs, dJ, dK);
+    if (rc != HFG_OK) return rc;
+    ms = 1e300;
+    for (int r = 0; r < reps; ++r) {
+      cudaEventRecord(ev.a, ctx->stream);
+      rc = jk_device_locked(ctx, &jo, nspin, dPt, dPs, dJ, dK);
+      if (rc != HFG_OK) return rc;
+      cudaEventRecord(ev.b, ctx->stream);
+      HFG_CUDA(ctx, cudaEventSynchronize(ev.b));
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev.a, ev.b);
+      ms = std::min(ms, (double)t);
+    }
+    return HFG_OK;
+  };
+  // energy error of (J, K) against (J64, K64); overwrites J and K
+  auto energy_error = [&](double& dE) -> int {
+    HFG_CUDA(ctx, cudaMemsetAsync(e.p, 0, sizeof(double), ctx->stream));
+    axpy_sub_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(J.p, J64.p, nn);
+    axpy_sub_kernel<<<nblk(nspin * nn), 256, 0, ctx->stream>>>(K.p, K64.p, nspin * nn);
+    wdot_kernel<<<296, 256, 0, ctx->stream>>>(dPt, J.p, nn, 0.5, e.p);
+    wdot_kernel<<<296, 256, 0, ctx->stream>>>(dPs, K.p, nspin * nn, nspin == 1 ? -0.25 : -0.5, e.p);
+    HFG_CUDA(ctx, cudaGetLastError());
+    HFG_CUDA(ctx, cudaMemcpyAsync(&dE, e.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return HFG_OK;
+  };
+  *res = hfg_autotune_result{};
+  hfg_jk_opts j64 = b;
+  j64.precision = HFG_FP64;
+  j64.prim_threshold = 0.0;
+  int rc = run(j64, J64.p, K64.p, 1, res->fp64_ms);
+  if (rc != HFG_OK) return rc;
+  res->best = j64;
+  res->best_ms = 1e300;
+  int k = 0;
+  for (int i = 0; i < o.n_fp32; ++i)
+    for (int j = 0; j < o.n_prim; ++j, ++k) {
+      hfg_jk_opts c = b;
+      c.precision = HFG_MIXED;
+      c.mixed_threshold = o.fp32_thresholds[i];
+      c.prim_threshold = o.prim_thresholds[j];
+      double ms = 0.0, dE = 0.0;
+      rc = run(c, J.p, K.p, o.repeats, ms);
+      if (rc != HFG_OK) return rc;
+      rc = energy_error(dE);
+      if (rc != HFG_OK) return rc;
+      res->ms[k] = ms;
+      res->energy_error[k] = dE;
+      if (std::fabs(dE) <= o.max_energy_error && ms < res->best_ms) {
+        res->best = c;
+        res->best_ms = ms;
+        res->best_energy_error = dE;
+        res->found = 1;
+      }
+    }
+  res->evaluated = k;
+  if (!res->found) res->best_ms = res->fp64_ms;
+  return HFG_OK;
 }
 
 int hfg_fma_peak(int device, int fp32, double* tflops) {

@@ -47,9 +47,9 @@ __global__ void __launch_bounds__(128) eri_packed_kernel(const JKEntry* __restri
 #pragma unroll
   for (int x = 0; x < C::NACC; ++x) acc[x] = 0.0;
   for (int ik = 0; ik < ket.npp; ++ik) {
-    const PrimRec64 Q = rec[ket.pp_off + ik];
+    const PrimRec64 Q = rec[ket.rec_off + (size_t)ik * ket.rec_stride];
     for (int ib = 0; ib < bra.npp; ++ib) {
-      const PrimRec64 P = rec[bra.pp_off + ib];
+      const PrimRec64 P = rec[bra.rec_off + (size_t)ib * bra.rec_stride];
       prim_quartet<LA, LB, LC, LD, double>(acc, P.p, P.inv_p, P.kp, -P.bp * bra.ABx, -P.bp * bra.ABy,
                                            -P.bp * bra.ABz, Q.p, Q.inv_p, Q.kp, -Q.bp * ket.ABx, -Q.bp * ket.ABy,
                                            -Q.bp * ket.ABz, ACx, ACy, ACz, sm);

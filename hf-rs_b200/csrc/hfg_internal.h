@@ -8,14 +8,19 @@ namespace hfg {
 constexpr int kLMax = 2;  // angular momentum built into the J/K kernels (s, p, d)
 
 // One shell pair, oriented so that la >= lb (and Ka >= Kb when la == lb).
-// 64 bytes.
+// 80 bytes.
 struct PairInfo {
   double Ax, Ay, Az;     // centre of shell a
   double ABx, ABy, ABz;  // A - B
   int ao_a, ao_b;        // first Cartesian function of shell a / b
-  int pp_off, npp;       // primitive pairs [pp_off, pp_off + npp), sorted by bound
+  int pp_off, npp;       // primitive pairs [pp_off, pp_off + npp) of the PrimPair table, sorted by bound
   int same;              // shells a and b are the same shell
   int cls;               // pair class index
+  // compact records (PrimRec64 / PrimRec32 / bounds) of primitive pair k of
+  // this shell pair: index rec_off + k * rec_stride.  The records of one pair
+  // class are interleaved (stride = pairs in the class), so the lanes of a
+  // warp holding consecutive pairs of a class read consecutive records.
+  int rec_off, rec_stride;
 };
 
 // One primitive pair.  64 bytes.  kp = c_a c_b exp(-mu |AB|^2) / p with the
@@ -30,8 +35,8 @@ struct PrimPair {
   double pad;
 };
 
-// Compact primitive-pair records read by the J/K kernels (structure of
-// arrays next to a float bound array): P - A = -bp * AB with bp = beta/p.
+// Compact primitive-pair records read by the J/K kernels (next to a float
+// bound array, same indexing): P - A = -bp * AB with bp = beta/p.
 struct __align__(32) PrimRec64 {
   double p, inv_p, kp, bp;
 };

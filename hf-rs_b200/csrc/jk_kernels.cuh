@@ -238,8 +238,8 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
       // primitive counts and consecutive records, so they start QPW * npp on)
       if (HFG_JK_PREFETCH && warp + 1 < t1 && kidx + QPW < ent.k_hi) {
         prefetch_l1(&a.pairs[kidx + QPW]);
-        prefetch_l1(RecOf<T>::get(a) + ket.pp_off + QPW * ket.npp);
-        prefetch_l1(a.pbound + ket.pp_off + QPW * ket.npp);
+        prefetch_l1(RecOf<T>::get(a) + ket.rec_off + QPW);
+        prefetch_l1(a.pbound + ket.rec_off + QPW);
       }
       DBlocks<LA, LB, LC, LD, NS, T> dblk;
       if (HFG_JK_HOIST_D && active && gl == 0) dblk.load(bra, ket, a);
@@ -253,11 +253,11 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
         const T ACx = (T)(bra.Ax - ket.Ax), ACy = (T)(bra.Ay - ket.Ay), ACz = (T)(bra.Az - ket.Az);
         const T bABx = (T)bra.ABx, bABy = (T)bra.ABy, bABz = (T)bra.ABz;
         const T kABx = (T)ket.ABx, kABy = (T)ket.ABy, kABz = (T)ket.ABz;
-        const Rec* __restrict__ br = RecOf<T>::get(a) + bra.pp_off;
-        const Rec* __restrict__ kr = RecOf<T>::get(a) + ket.pp_off;
-        const float* __restrict__ bb = a.pbound + bra.pp_off;
-        const float* __restrict__ kb = a.pbound + ket.pp_off;
-        const int nb = bra.npp, nk = ket.npp;
+        const Rec* __restrict__ br = RecOf<T>::get(a) + bra.rec_off;
+        const Rec* __restrict__ kr = RecOf<T>::get(a) + ket.rec_off;
+        const float* __restrict__ bb = a.pbound + bra.rec_off;
+        const float* __restrict__ kb = a.pbound + ket.rec_off;
+        const int nb = bra.npp, nk = ket.npp, bs = bra.rec_stride, ks = ket.rec_stride;
         // screening products in FP32 (bounds are stored as floats; count_kernel
         // evaluates the same products)
         const float eps = (float)a.prim_eps;
@@ -270,18 +270,18 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
           int lo = 0;
           while (lo < nke) {
             const int mid = (lo + nke) >> 1;
-            if (kb[mid] * bmax >= eps) lo = mid + 1; else nke = mid;
+            if (kb[mid * ks] * bmax >= eps) lo = mid + 1; else nke = mid;
           }
         }
-        Rec Qn = kr[gl < nk ? gl : 0];
-        float qbn = kb[gl < nk ? gl : 0];
+        Rec Qn = kr[(gl < nk ? gl : 0) * ks];
+        float qbn = kb[(gl < nk ? gl : 0) * ks];
         for (int ik = gl; ik < nke; ik += G) {
           const Rec Q = Qn;
           const float qb = qbn;
           if (!HFG_JK_NKE_SEARCH && qb * bmax < eps) break;
           if (ik + G < nke) {
-            Qn = kr[ik + G];
-            qbn = kb[ik + G];
+            Qn = kr[(ik + G) * ks];
+            qbn = kb[(ik + G) * ks];
           }
           const T QCx = -Q.bp * kABx, QCy = -Q.bp * kABy, QCz = -Q.bp * kABz;
           int ib = 0;
@@ -289,18 +289,18 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
             // two independent primitive quartets per step (bra primitive pairs
             // are sorted by bound: if the second survives, so does the first)
             for (; ib + 1 < nb; ib += 2) {
-              if (bb[ib + 1] * qb < eps) break;
-              const Rec P0 = br[ib], P1 = br[ib + 1];
+              if (bb[(ib + 1) * bs] * qb < eps) break;
+              const Rec P0 = br[ib * bs], P1 = br[(ib + 1) * bs];
               prim_quartet<LA, LB, LC, LD, T>(acc, P0.p, P0.inv_p, P0.kp, -P0.bp * bABx, -P0.bp * bABy,
                                               -P0.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
               prim_quartet<LA, LB, LC, LD, T>(acc, P1.p, P1.inv_p, P1.kp, -P1.bp * bABx, -P1.bp * bABy,
                                               -P1.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
             }
           }
-          Rec P = br[ib < nb ? ib : 0];
+          Rec P = br[(ib < nb ? ib : 0) * bs];
           for (; ib < nb; ++ib) {
-            const Rec Pn = br[ib + 1 < nb ? ib + 1 : ib];
-            if (bb[ib] * qb < eps) break;
+            const Rec Pn = br[(ib + 1 < nb ? ib + 1 : ib) * bs];
+            if (bb[ib * bs] * qb < eps) break;
             prim_quartet<LA, LB, LC, LD, T>(acc, P.p, P.inv_p, P.kp, -P.bp * bABx, -P.bp * bABy, -P.bp * bABz, Q.p,
                                             Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
             P = Pn;

@@ -750,6 +750,9 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   hfg_jk_opts jo = o->jk;
   hfg_jk_opts jo64 = o->jk;
   jo64.precision = HFG_FP64;
+  // the refinement and final builds keep primitive screening at 1e-15 at most
+  // (the mixed phase may use a looser, autotuned one)
+  jo64.prim_threshold = std::min(jo64.prim_threshold, 1e-15);
   // Incremental builds in the mixed phase: J/K are linear in the density, so
   // J(P) = J(P_full) + J(P - P_full) summed over the builds since the last
   // full one, and the change only needs the quartets with

@@ -32,14 +32,14 @@ __global__ void count_kernel(const JKEntry* __restrict__ entries, const long lon
     // one, then bra primitive pairs while the product stays above eps
     // (FP32 products, as in the kernels)
     const float feps = (float)eps;
-    const float bmax = pbound[b.pp_off];
+    const float bmax = pbound[b.rec_off];
     for (int ik = 0; ik < q.npp; ++ik) {
-      const float qb = pbound[q.pp_off + ik];
+      const float qb = pbound[q.rec_off + (size_t)ik * q.rec_stride];
       if (qb * bmax < feps) break;
       int l = 0, h = b.npp;  // bounds sorted descending
       while (l < h) {
         const int m = (l + h) >> 1;
-        if (pbound[b.pp_off + m] * qb >= feps) l = m + 1; else h = m;
+        if (pbound[b.rec_off + (size_t)m * b.rec_stride] * qb >= feps) l = m + 1; else h = m;
       }
       c += (unsigned long long)l;
     }

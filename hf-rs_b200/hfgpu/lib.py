@@ -43,6 +43,9 @@ class JKOptions(ctypes.Structure):
         o.mixed_threshold = 0.0 if mixed is None else mixed
         return o
 
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
 
 class SCFOptions(ctypes.Structure):
     _fields_ = [("natom", ctypes.c_int), ("positions", ctypes.POINTER(ctypes.c_double)),
@@ -100,6 +103,18 @@ class JKStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class AutotuneOptions(ctypes.Structure):
+    _fields_ = [("fp32_thresholds", ctypes.c_double * 8), ("n_fp32", ctypes.c_int),
+                ("prim_thresholds", ctypes.c_double * 8), ("n_prim", ctypes.c_int),
+                ("max_energy_error", ctypes.c_double), ("repeats", ctypes.c_int)]
+
+
+class AutotuneResult(ctypes.Structure):
+    _fields_ = [("best", JKOptions), ("found", ctypes.c_int), ("best_ms", ctypes.c_double),
+                ("best_energy_error", ctypes.c_double), ("fp64_ms", ctypes.c_double), ("evaluated", ctypes.c_int),
+                ("ms", ctypes.c_double * 64), ("energy_error", ctypes.c_double * 64)]
+
+
 _lib = None
 DP = ctypes.POINTER(ctypes.c_double)
 VP = ctypes.c_void_p
@@ -139,6 +154,8 @@ def load_library():
     L.hfg_fock_rhf.argtypes = [VP, P(JKOptions), DP, DP, DP]
     L.hfg_fock_uhf.argtypes = [VP, P(JKOptions), DP, DP, DP, DP, DP]
     L.hfg_jk_last_stats.argtypes = [VP, P(JKStats)]
+    L.hfg_autotune_opts_default.argtypes = [P(AutotuneOptions)]
+    L.hfg_jk_autotune.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, P(AutotuneOptions), P(AutotuneResult)]
     L.hfg_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, DP]
     L.hfg_scf_opts_default.argtypes = [P(SCFOptions)]
     L.hfg_df_build.argtypes = [VP, P(HfgBasis), ctypes.c_double, ctypes.c_double, ctypes.c_int, P(VP)]
@@ -348,6 +365,37 @@ class Context:
         s = JKStats()
         self._check(self.lib.hfg_jk_last_stats(self.h, ctypes.byref(s)))
         return s.as_dict()
+
+    def autotune(self, d_total, d_spin, nspin=1, base=None, fp32=(), prim=(), max_energy_error=None, repeats=None):
+        """hfg_jk_autotune on device densities (integer pointers): returns the
+        chosen JKOptions and a report of every candidate."""
+        o = AutotuneOptions()
+        self.lib.hfg_autotune_opts_default(ctypes.byref(o))
+        if fp32:
+            o.n_fp32 = len(fp32)
+            for i, v in enumerate(fp32):
+                o.fp32_thresholds[i] = v
+        if prim:
+            o.n_prim = len(prim)
+            for i, v in enumerate(prim):
+                o.prim_thresholds[i] = v
+        if max_energy_error is not None:
+            o.max_energy_error = max_energy_error
+        if repeats is not None:
+            o.repeats = repeats
+        r = AutotuneResult()
+        b = base or JKOptions.make()
+        self._check(self.lib.hfg_jk_autotune(self.h, ctypes.byref(b), nspin, d_total, d_spin, ctypes.byref(o),
+                                             ctypes.byref(r)))
+        fl = [o.fp32_thresholds[i] for i in range(o.n_fp32)]
+        pl = [o.prim_thresholds[i] for i in range(o.n_prim)]
+        cands = [{"fp32_threshold": f, "prim_threshold": p, "ms": r.ms[k], "energy_error": r.energy_error[k]}
+                 for k, (f, p) in enumerate((f, p) for f in fl for p in pl)]
+        best = JKOptions()
+        ctypes.memmove(ctypes.byref(best), ctypes.byref(r.best), ctypes.sizeof(JKOptions))
+        return best, {"found": bool(r.found), "best_ms": r.best_ms, "best_energy_error": r.best_energy_error,
+                      "fp64_ms": r.fp64_ms, "max_energy_error": o.max_energy_error, "candidates": cands,
+                      "best": best.as_dict()}
 
 
 HFG_DF_FP64, HFG_DF_FP32, HFG_DF_BF16 = 0, 1, 2

@@ -156,6 +156,42 @@ typedef struct {
 } hfg_jk_stats;
 int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* stats);
 
+/*
+ * Autotuner of the mixed-precision J/K build (no hf-rs counterpart: hf-rs
+ * has a single FP64 path).  For the given densities (device pointers, as
+ * hfg_jk_device) it builds J/K once in plain FP64 (Schwarz screening only,
+ * the reference's arithmetic) and then, for every pair of FP32 threshold
+ * and primitive threshold in the candidate lists, times `repeats` mixed
+ * builds on the device (CUDA events on the context stream; the first build
+ * of each candidate, which makes its plan, is not timed) and evaluates the
+ * energy error of the build,
+ *   dE = 1/2 sum P_total (J - J64) - w sum_s P_s (K_s - K64_s),
+ * w = 1/4 for RHF (nspin 1) and 1/2 for UHF.  The fastest candidate with
+ * |dE| <= max_energy_error is returned in `best` (schwarz_threshold from
+ * `base`); if none qualifies, `best` is the FP64 options of `base` and
+ * `found` is 0.  Empty candidate lists use 1e-9, 1e-8, 1e-7, 1e-6 (FP32) and
+ * 1e-15, 1e-14, 1e-13 (primitives); the default budget is 5e-9 Eh.
+ */
+typedef struct {
+  double fp32_thresholds[8];
+  int n_fp32;
+  double prim_thresholds[8];
+  int n_prim;
+  double max_energy_error;
+  int repeats;
+} hfg_autotune_opts;
+typedef struct {
+  hfg_jk_opts best;
+  int found;
+  double best_ms, best_energy_error;
+  double fp64_ms;                   /* the plain FP64 build */
+  int evaluated;
+  double ms[64], energy_error[64];  /* per candidate, FP32-threshold-major order */
+} hfg_autotune_result;
+void hfg_autotune_opts_default(hfg_autotune_opts* opts);
+int hfg_jk_autotune(hfg_ctx* ctx, const hfg_jk_opts* base, int nspin, const double* d_P_total,
+                    const double* d_P_spin, const hfg_autotune_opts* opts, hfg_autotune_result* result);
+
 /* Density fitting (src/df.rs, src/hf_variants/ri_df_hf.rs). */
 typedef enum { HFG_DF_FP64 = 0, HFG_DF_FP32 = 1, HFG_DF_BF16 = 2 } hfg_df_precision;
 typedef struct hfg_df hfg_df;

@@ -149,3 +149,22 @@ def test_eri_packed_rejects_wrong_length():
     ctx = Context(CartesianBasis.build(water_cluster(1), "sto-3g"))
     with pytest.raises(HfgError, match="INVALID_INPUT"):
         ctx.eri_packed(1e-12, length=10)
+
+
+def test_autotune_picks_fastest_within_energy_budget():
+    # the autotuner's choice meets its energy budget when checked independently
+    import torch
+    atoms = water_cluster(4)
+    ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
+    P = ctx.scf(spherical=True, tol=1e-10, max_iter=3, want=("P",))["P"][0]
+    dP = torch.from_numpy(np.ascontiguousarray(P)).to(torch.device("cuda", 0))
+    torch.cuda.synchronize()  # the context runs on its own stream
+    best, rep = ctx.autotune(dP.data_ptr(), dP.data_ptr(), max_energy_error=5e-9, repeats=1)
+    assert rep["found"] and len(rep["candidates"]) == 12
+    ok = [c for c in rep["candidates"] if abs(c["energy_error"]) <= 5e-9]
+    assert rep["best_ms"] == min(c["ms"] for c in ok)
+    J0, K0 = ctx.jk(P, opts=JKOptions.make(prim=0.0))
+    J1, K1 = ctx.jk(P, opts=best)
+    dE = 0.5 * np.sum(P * (J1 - J0)) - 0.25 * np.sum(P * (K1[0] - K0[0]))
+    assert abs(dE - rep["best_energy_error"]) < 1e-10
+    assert abs(dE) <= 5e-9
