@@ -374,14 +374,18 @@ def run_ours(args):
     p32 = fma_peak_tflops(local, True)
     t_step = tot_mixed / args.steps / 1000.0
     pipe_frac = (stats_mixed["wmd_flops_fp64"] / (p64 * 1e12) + stats_mixed["wmd_flops_fp32"] / (p32 * 1e12)) / t_step
+    # DRAM bytes of one mixed build from the committed ncu summary (captured
+    # on (H2O)32; dominated by register spills of the L >= 4 classes)
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "jk_kernels_h2o64.txt")
+    prof = os.path.join(ROOT, "profiles", "jk_kernel_1000_h2o32.md")
     if os.path.exists(prof):
         for ln in open(prof):
-            if ln.startswith("traffic_bytes_per_build:"):
+            if ln.startswith("traffic_bytes_per_mixed_build_h2o32:"):
                 traffic = float(ln.split(":")[1])
     roofline = {"bound": "fp64", "achieved": pipe_frac * p64, "peak": p64, "unit": "TFLOP/s", "frac": pipe_frac,
                 "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read+write of one autotuned mixed build of (H2O)32 (the "
+                                  "full-size capture is not made); mostly register spills of the L>=4 classes",
                 "peak_source": "measured FMA chains on this device (hfg_fma_peak); FP32 work weighted by the "
                                "measured FP32 peak %.1f TFLOP/s" % p32,
                 "work_unit": "McMurchie-Davidson flops per evaluated primitive quartet (hf-rs loops), "

@@ -160,16 +160,19 @@ __device__ __forceinline__ void digest(const DT* __restrict__ w, const PairInfo&
 // HFG_JK_MIN_BLOCKS_F64 / _F32 macros override the table for tuning builds.
 template <int LA, int LB, int LC, int LD, typename T> struct MinBlocks {
   static constexpr int code = LA * 1000 + LB * 100 + LC * 10 + LD;
+  static constexpr int L = LA + LB + LC + LD;
 #ifdef HFG_JK_MIN_BLOCKS_F64
   static constexpr int f64 = HFG_JK_MIN_BLOCKS_F64;
 #else
-  static constexpr int f64 = 2;
+  static constexpr int f64 = L >= 5 ? 1 : 2;
 #endif
 #ifdef HFG_JK_MIN_BLOCKS_F32
   static constexpr int f32 = HFG_JK_MIN_BLOCKS_F32;
 #else
-  static constexpr int f32 =
-      (code == 0 || code == 1000 || code == 1010) ? 4 : (code == 1100 || code == 2000 || code == 2100) ? 3 : 2;
+  static constexpr int f32 = (code == 0 || code == 1000 || code == 1010)   ? 4
+                             : (code == 1100 || code == 2000 || code == 2100) ? 3
+                             : L >= 6                                         ? 1
+                                                                              : 2;
 #endif
   static constexpr int value = sizeof(T) == 4 ? f32 : f64;
 };
@@ -323,7 +326,8 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
         if (bra.same) deg *= (T)0.5;
         if (ket.same) deg *= (T)0.5;
         if (kidx == ent.bra) deg *= (T)0.5;
-        T w[C::NOUT];
+        // scaled in place (a second block-sized array would double the
+        // per-thread footprint of the large classes)
 #pragma unroll
         for (int i = 0; i < NA; ++i)
 #pragma unroll
@@ -333,10 +337,9 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
 #pragma unroll
               for (int l = 0; l < ND; ++l) {
                 const int x = ((i * NB + j) * NC + k) * ND + l;
-                w[x] = out[x] * (deg * (T)(comp_scale(LA, i) * comp_scale(LB, j) * comp_scale(LC, k) *
-                                           comp_scale(LD, l)));
+                out[x] *= deg * (T)(comp_scale(LA, i) * comp_scale(LB, j) * comp_scale(LC, k) * comp_scale(LD, l));
               }
-        digest<LA, LB, LC, LD, NS, T>(w, bra, ket, a, dblk, jab);
+        digest<LA, LB, LC, LD, NS, T>(out, bra, ket, a, dblk, jab);
       } else {
 #pragma unroll
         for (int x = 0; x < NAB; ++x) jab[x] = (T)0;
