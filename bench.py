@@ -442,13 +442,13 @@ def measure_serving(args):
     {1..serve_max_waters}, bases uniform over STO-3G / 6-31G* / cc-pVDZ, 10%
     UHF doublets).  Sequential: one FP64 solve at a time.  Served: 8 slots,
     mixed precision with FP64 refinement, all jobs submitted at once (an
-    arrival rate above capacity)."""
+    arrival rate above capacity); jobs under 256 basis functions run FP64."""
     from hfgpu.serve import MIXED, build_inputs, make_stream, run_stream, summarize
     jobs = make_stream(args.serve_jobs, rate=1000.0, max_waters=args.serve_max_waters, seed=4242)
     inputs = build_inputs(jobs)
     seq, span_seq = run_stream(jobs, slots=1, budget_bytes=120 << 30, honour_arrivals=False, inputs=inputs)
     srv, span_srv = run_stream(jobs, slots=8, budget_bytes=120 << 30, honour_arrivals=False, inputs=inputs,
-                               jk=MIXED)
+                               jk=MIXED, mixed_min_ao=256)
     a, b = summarize(seq, span_seq), summarize(srv, span_srv)
     de = max(abs(x["energy"] - y["energy"]) for x, y in zip(seq, srv) if x["status"] == 0 and y["status"] == 0)
     return {"sample": "%d jobs, waters 1..%d, STO-3G/6-31G*/cc-pVDZ, 10%% UHF" % (len(jobs), args.serve_max_waters),

@@ -15,6 +15,8 @@
 #include <cublas_v2.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <cstdlib>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -179,9 +181,12 @@ int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, doubl
     CK(cudaMemcpyAsync(V.p, Vh.data(), (size_t)naux * rank * 8, cudaMemcpyHostToDevice, st));
   }
 
-  // significant orbital shell pairs and their unique AO-pair columns
-  std::map<std::pair<int, int>, std::vector<int>> bra_by_class;
-  std::map<std::pair<int, int>, std::vector<long long>> col_by_class;
+  // significant orbital shell pairs (in pair order) and their unique AO-pair columns
+  struct SigPair {
+    int pair, la, lb;
+    long long col;
+  };
+  std::vector<SigPair> sig;
   std::vector<int2> colmn;
   long long ncol = 0;
   for (size_t i = 0; i < ctx->h_pairs.size(); ++i) {
@@ -189,8 +194,7 @@ int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, doubl
     const PairInfo& pi = ctx->h_pairs[i];
     const PairClass& c = ctx->classes[pi.cls];
     const int na = (c.la + 1) * (c.la + 2) / 2, nb = (c.lb + 1) * (c.lb + 2) / 2;
-    bra_by_class[{c.la, c.lb}].push_back((int)i);
-    col_by_class[{c.la, c.lb}].push_back(ncol);
+    sig.push_back({(int)i, c.la, c.lb, ncol});
     for (int a = 0; a < na; ++a)
       for (int b = 0; b < nb; ++b) {
         if (pi.same && b > a) continue;
@@ -201,43 +205,74 @@ int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, doubl
   df->ncol = ncol;
   CK(df->colmn.alloc(ncol));
   CK(cudaMemcpyAsync(df->colmn.p, colmn.data(), ncol * sizeof(int2), cudaMemcpyHostToDevice, st));
-  // (P|mn) for all columns (rows = auxiliary functions), then B = Xm^T (P|mn)
-  DevBuf<double> T3;
-  CK(T3.alloc((size_t)naux * ncol));
-  for (auto& bc : bra_by_class) {
-    DevBuf<int> bidx;
-    DevBuf<long long> bcol;
-    CK(bidx.alloc(bc.second.size()));
-    CK(bcol.alloc(bc.second.size()));
-    CK(cudaMemcpyAsync(bidx.p, bc.second.data(), bc.second.size() * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(bcol.p, col_by_class[bc.first].data(), bc.second.size() * 8, cudaMemcpyHostToDevice, st));
-    for (auto& kk : aux_by_l) {
-      Df3cArgs a{ctx->d_pairs.p, ctx->d_prims.p, bidx.p, bcol.p, (int)bc.second.size(), dup.p, dupr.p,
-                 aux_idx[kk.first].p, (int)kk.second.size(), ctx->d_boys64.p, ctx->d_expt64.p, T3.p, ncol};
-      CK(launch_df3c(bc.first.first, bc.first.second, kk.first, a, st));
-    }
-    CK(cudaStreamSynchronize(st));
-  }
   if (cublasCreate(&df->blas) != CUBLAS_STATUS_SUCCESS) return set_error(ctx, HFG_ERR_CUDA, "cublasCreate");
   cublasSetStream(df->blas, st);
-  CK(df->B64.alloc((size_t)rank * ncol));
-  {
-    // column-major view: T3c (ncol x naux), Xm (naux x rank) -> Bc (ncol x rank) = B row-major [rank][ncol]
-    const double one = 1.0, zero = 0.0;
-    if (cublasDgemm(df->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)ncol, rank, naux, &one, T3.p, (int)ncol, V.p, naux, &zero,
-                    df->B64.p, (int)ncol) != CUBLAS_STATUS_SUCCESS)
-      return set_error(ctx, HFG_ERR_CUDA, "B = X^T (P|mn) GEMM failed");
+  // the stored factor B (row-major [rank][ncol]) in its storage precision
+  if (storage == HFG_DF_FP64) CK(df->B64.alloc((size_t)rank * ncol));
+  else if (storage == HFG_DF_FP32) CK(df->B32.alloc((size_t)rank * ncol));
+  else CK(df->B16.alloc((size_t)rank * ncol));
+  // (P|mn) and B = Xm^T (P|mn) over chunks of consecutive columns, so that
+  // only one chunk of the FP64 three-centre integrals (naux x width) and of
+  // the FP64 product (rank x width) is held at a time: about 8 GiB, or a
+  // quarter of the free device memory if that is less
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const double budget = std::min(8.0 * (1ull << 30), 0.25 * (double)free_b);
+  const long long per_col = 8LL * (naux + (storage == HFG_DF_FP64 ? 0 : rank));
+  long long width_max = std::max(256LL, std::min(ncol, (long long)(budget / (double)per_col)));
+  // HFG_DF_CHUNK_COLS caps the chunk width (tests use it to exercise chunking
+  // on small systems)
+  if (const char* ev = getenv("HFG_DF_CHUNK_COLS")) {
+    const long long v = atoll(ev);
+    if (v > 0) width_max = std::min(width_max, std::max(64LL, v));
   }
-  T3.release();
-  if (storage == HFG_DF_FP32) {
-    CK(df->B32.alloc((size_t)rank * ncol));
-    CK(launch_convert(1, df->B64.p, df->B32.p, (long long)rank * ncol, st));
-  } else if (storage == HFG_DF_BF16) {
-    CK(df->B16.alloc((size_t)rank * ncol));
-    CK(launch_convert(2, df->B64.p, df->B16.p, (long long)rank * ncol, st));
+  DevBuf<double> T3, Bt;
+  CK(T3.alloc((size_t)naux * std::min(width_max + 64, ncol)));
+  if (storage != HFG_DF_FP64) CK(Bt.alloc((size_t)rank * std::min(width_max + 64, ncol)));
+  size_t p0 = 0;
+  while (p0 < sig.size()) {
+    // pairs [p0, p1) whose columns fit in the chunk (one pair has at most 36)
+    const long long c0 = sig[p0].col;
+    size_t p1 = p0;
+    while (p1 < sig.size() && sig[p1].col - c0 < width_max) ++p1;
+    const long long c1 = p1 < sig.size() ? sig[p1].col : ncol;
+    const int w = (int)(c1 - c0);
+    std::map<std::pair<int, int>, std::pair<std::vector<int>, std::vector<long long>>> by_class;
+    for (size_t k = p0; k < p1; ++k) {
+      auto& e = by_class[{sig[k].la, sig[k].lb}];
+      e.first.push_back(sig[k].pair);
+      e.second.push_back(sig[k].col - c0);
+    }
+    for (auto& bc : by_class) {
+      DevBuf<int> bidx;
+      DevBuf<long long> bcol;
+      CK(bidx.alloc(bc.second.first.size()));
+      CK(bcol.alloc(bc.second.second.size()));
+      CK(cudaMemcpyAsync(bidx.p, bc.second.first.data(), bc.second.first.size() * 4, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(bcol.p, bc.second.second.data(), bc.second.second.size() * 8, cudaMemcpyHostToDevice, st));
+      for (auto& kk : aux_by_l) {
+        Df3cArgs a{ctx->d_pairs.p, ctx->d_prims.p, bidx.p, bcol.p, (int)bc.second.first.size(), dup.p, dupr.p,
+                   aux_idx[kk.first].p, (int)kk.second.size(), ctx->d_boys64.p, ctx->d_expt64.p, T3.p, w};
+        CK(launch_df3c(bc.first.first, bc.first.second, kk.first, a, st));
+      }
+      CK(cudaStreamSynchronize(st));  // the index buffers are released at the end of this scope
+    }
+    // column-major view: T3c (w x naux, ld w) times Xm (naux x rank) gives the
+    // chunk's columns of B (row-major [rank][ncol] = column-major ncol x rank)
+    const double one = 1.0, zero = 0.0;
+    double* dst = storage == HFG_DF_FP64 ? df->B64.p + c0 : Bt.p;
+    const int ldc = storage == HFG_DF_FP64 ? (int)ncol : w;
+    if (cublasDgemm(df->blas, CUBLAS_OP_N, CUBLAS_OP_N, w, rank, naux, &one, T3.p, w, V.p, naux, &zero, dst, ldc) !=
+        CUBLAS_STATUS_SUCCESS)
+      return set_error(ctx, HFG_ERR_CUDA, "B = X^T (P|mn) GEMM failed");
+    if (storage != HFG_DF_FP64)
+      CK(launch_convert_cols(storage == HFG_DF_FP32 ? 1 : 2, Bt.p, w, rank,
+                             storage == HFG_DF_FP32 ? (void*)df->B32.p : (void*)df->B16.p, ncol, c0, st));
+    p0 = p1;
   }
   CK(cudaStreamSynchronize(st));
-  if (storage != HFG_DF_FP64) df->B64.release();
+  T3.release();
+  Bt.release();
   *out = df.release();
 #undef CK
   return HFG_OK;
@@ -286,10 +321,12 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
     rc = cuda_check(ctx, (call), #call); \
     if (rc != HFG_OK) return rc;         \
   } while (0)
-  if (df->storage == HFG_DF_FP64 && mma != HFG_DF_FP64) mma = HFG_DF_FP64;
-  if (df->storage == HFG_DF_FP32 && mma == HFG_DF_FP64) mma = HFG_DF_FP32;
-  if (df->storage == HFG_DF_BF16) mma = HFG_DF_BF16;
-  if (df->storage == HFG_DF_FP32 && mma == HFG_DF_BF16) mma = HFG_DF_FP32;
+  // arithmetic of the K GEMMs: FP64 storage always FP64; FP32 storage TF32
+  // or BF16 tensor cores (the factor rounded to BF16 while unpacking) or FP64
+  // on the converted factor; BF16 storage BF16 tensor cores or FP64 on the
+  // converted factor
+  if (df->storage == HFG_DF_FP64) mma = HFG_DF_FP64;
+  if (df->storage == HFG_DF_BF16 && mma == HFG_DF_FP32) mma = HFG_DF_BF16;
   const double one = 1.0, zero = 0.0, two = 2.0;
   // P = 2 C C^T
   CK(df->P.alloc(nn));
@@ -305,46 +342,20 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
     cublasDgemv(df->blas, CUBLAS_OP_T, (int)ncol, rank, &one, df->B64.p, (int)ncol, df->pvec.p, 1, &zero, df->gam.p, 1);
     cublasDgemv(df->blas, CUBLAS_OP_N, (int)ncol, rank, &one, df->B64.p, (int)ncol, df->gam.p, 1, &zero, df->jcol.p, 1);
   } else {
-    // FP32 accumulation of the packed contractions on the stored precision
+    // the stored FP32 / BF16 factor with FP64 accumulation (J is
+    // memory-bound; the density is not rounded)
     const bool bf = df->storage == HFG_DF_BF16;
-    const void* Bp = bf ? (const void*)df->B16.p : (const void*)df->B32.p;
-    const cudaDataType bt = bf ? CUDA_R_16BF : CUDA_R_32F;
-    CK(df->pvec32.alloc(ncol));
-    CK(df->gam32.alloc(rank));
-    CK(df->jcol32.alloc(ncol));
-    DevBuf<__nv_bfloat16> pv16, g16;
-    CK(launch_convert(1, df->pvec.p, df->pvec32.p, ncol, st));
-    const void* pv = df->pvec32.p;
-    cudaDataType pt = CUDA_R_32F;
-    if (bf) {
-      CK(pv16.alloc(ncol));
-      CK(launch_convert(2, df->pvec.p, pv16.p, ncol, st));
-      pv = pv16.p;
-      pt = CUDA_R_16BF;
-    }
-    rc = gemm_ex(ctx, df->blas, CUBLAS_OP_T, CUBLAS_OP_N, rank, 1, (int)ncol, Bp, bt, (int)ncol, pv, pt, (int)ncol,
-                 0.0f, df->gam32.p, rank, CUBLAS_COMPUTE_32F);
-    if (rc != HFG_OK) return rc;
-    const void* gv = df->gam32.p;
-    cudaDataType gt = CUDA_R_32F;
-    if (bf) {
-      CK(g16.alloc(rank));
-      CK(launch_convert_f32(2, df->gam32.p, g16.p, rank, st));
-      gv = g16.p;
-      gt = CUDA_R_16BF;
-    }
-    rc = gemm_ex(ctx, df->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)ncol, 1, rank, Bp, bt, (int)ncol, gv, gt, rank, 0.0f,
-                 df->jcol32.p, (int)ncol, CUBLAS_COMPUTE_32F);
-    if (rc != HFG_OK) return rc;
-    CK(cudaMemsetAsync(df->jcol.p, 0, ncol * 8, st));
-    CK(launch_accumulate_f32(df->jcol.p, df->jcol32.p, 1.0, ncol, st));
+    CK(launch_df_j(bf ? 2 : 1, bf ? (const void*)df->B16.p : (const void*)df->B32.p, ncol, rank, df->pvec.p,
+                   df->gam.p, df->jcol.p, st));
   }
   CK(cudaMemsetAsync(dJ, 0, nn * 8, st));
   CK(launch_unpack_j(df->jcol.p, df->colmn.p, ncol, n, dJ, st));
 
   // K: chunks of qc auxiliary functions
   const size_t esz = mma == HFG_DF_FP64 ? 8 : (mma == HFG_DF_FP32 ? 4 : 2);
-  const size_t budget = (size_t)1 << 30;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t budget = std::max<size_t>((size_t)64 << 20, std::min<size_t>((size_t)4 << 30, free_b / 4));
   int qc = (int)std::max<size_t>(1, std::min<size_t>((size_t)rank, budget / ((size_t)nn * esz)));
   CK(df->dense.alloc((size_t)qc * nn * esz));
   CK(cudaMemsetAsync(dK, 0, nn * 8, st));
@@ -353,7 +364,11 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
     for (int q0 = 0; q0 < rank; q0 += qc) {
       const int qn = std::min(qc, rank - q0);
       CK(cudaMemsetAsync(df->dense.p, 0, (size_t)qn * nn * 8, st));
-      CK(launch_df_unpack(0, df->B64.p, ncol, df->colmn.p, ncol, q0, qn, n, df->dense.p, st));
+      // FP64 arithmetic on the stored factor, converted while unpacking
+      const int um = df->storage == HFG_DF_FP64 ? 0 : (df->storage == HFG_DF_FP32 ? 3 : 4);
+      const void* Bs = df->storage == HFG_DF_FP64 ? (const void*)df->B64.p
+                       : df->storage == HFG_DF_FP32 ? (const void*)df->B32.p : (const void*)df->B16.p;
+      CK(launch_df_unpack(um, Bs, ncol, df->colmn.p, ncol, q0, qn, n, df->dense.p, st));
       const double* Bd = (const double*)df->dense.p;
       // T^T (nocc x n*qn) = C^T (nocc x n) * Bd2^T (n x n*qn)
       cublasDgemm(df->blas, CUBLAS_OP_T, CUBLAS_OP_N, nocc, n * qn, n, &one, dC, n, Bd, n, &zero, df->T64.p, nocc);
@@ -379,7 +394,7 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
       Cin = df->Cf.p;
     }
     const void* Bsrc = df->storage == HFG_DF_BF16 ? (const void*)df->B16.p : (const void*)df->B32.p;
-    const int umode = df->storage == HFG_DF_BF16 ? 2 : 1;
+    const int umode = df->storage == HFG_DF_BF16 ? 2 : (bf ? 5 : 1);
     for (int q0 = 0; q0 < rank; q0 += qc) {
       const int qn = std::min(qc, rank - q0);
       CK(cudaMemsetAsync(df->dense.p, 0, (size_t)qn * nn * esz, st));

@@ -179,9 +179,61 @@ cudaError_t launch_df_unpack(int mode, const void* B, long long ldb, const int2*
                                                            (double*)out);
   else if (mode == 1)
     df_unpack_kernel<float, float><<<grid, 256, 0, st>>>((const float*)B, ldb, colmn, ncol, q0, qc, n, (float*)out);
-  else
+  else if (mode == 2)
     df_unpack_kernel<__nv_bfloat16, __nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)B, ldb, colmn, ncol,
                                                                          q0, qc, n, (__nv_bfloat16*)out);
+  else if (mode == 5)
+    df_unpack_kernel<__nv_bfloat16, float><<<grid, 256, 0, st>>>((const float*)B, ldb, colmn, ncol, q0, qc, n,
+                                                                  (__nv_bfloat16*)out);
+  else if (mode == 3)
+    df_unpack_kernel<double, float><<<grid, 256, 0, st>>>((const float*)B, ldb, colmn, ncol, q0, qc, n, (double*)out);
+  else
+    df_unpack_kernel<double, __nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)B, ldb, colmn, ncol, q0, qc,
+                                                                  n, (double*)out);
+  return cudaGetLastError();
+}
+
+// J contractions on a stored FP32 / BF16 factor with FP64 accumulation
+// (memory-bound: each reads B once): gam[q] = sum_c B[q][c] p[c], one block
+// per auxiliary index; j[c] = sum_q B[q][c] gam[q], one thread per column.
+template <typename TB>
+__global__ void df_gamma_kernel(const TB* __restrict__ B, long long ncol, const double* __restrict__ p,
+                                double* __restrict__ gam) {
+  const long long row = (long long)blockIdx.x * ncol;
+  double s = 0.0;
+  for (long long c = threadIdx.x; c < ncol; c += blockDim.x) s += (double)(float)B[row + c] * p[c];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  __shared__ double part[8];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += part[k];
+    gam[blockIdx.x] = t;
+  }
+}
+
+template <typename TB>
+__global__ void df_jcol_kernel(const TB* __restrict__ B, long long ncol, int rank, const double* __restrict__ gam,
+                               double* __restrict__ j) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncol; c += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < rank; ++q) s += (double)(float)B[(long long)q * ncol + c] * gam[q];
+    j[c] = s;
+  }
+}
+
+cudaError_t launch_df_j(int mode, const void* B, long long ncol, int rank, const double* p, double* gam, double* j,
+                        cudaStream_t st) {
+  if (ncol <= 0 || rank <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)std::min<long long>((ncol + 255) / 256, 148 * 16);
+  if (mode == 1) {
+    df_gamma_kernel<float><<<rank, 256, 0, st>>>((const float*)B, ncol, p, gam);
+    df_jcol_kernel<float><<<grid, 256, 0, st>>>((const float*)B, ncol, rank, gam, j);
+  } else {
+    df_gamma_kernel<__nv_bfloat16><<<rank, 256, 0, st>>>((const __nv_bfloat16*)B, ncol, p, gam);
+    df_jcol_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)B, ncol, rank, gam, j);
+  }
   return cudaGetLastError();
 }
 
@@ -223,6 +275,28 @@ cudaError_t launch_convert(int mode, const double* in, void* out, long long len,
   if (mode == 0) convert_kernel<double><<<grid, 256, 0, st>>>(in, (double*)out, len);
   else if (mode == 1) convert_kernel<float><<<grid, 256, 0, st>>>(in, (float*)out, len);
   else convert_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(in, (__nv_bfloat16*)out, len);
+  return cudaGetLastError();
+}
+
+// out[r * ldo + c0 + j] = in[r * w + j] for r < rows, j < w (a chunk of B's
+// columns, FP64 GEMM output, into the stored factor)
+template <typename TO>
+__global__ void convert_cols_kernel(const double* __restrict__ in, int w, long long rows, TO* __restrict__ out,
+                                    long long ldo, long long c0) {
+  const long long len = rows * w;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x) {
+    const long long r = i / w, j = i - r * w;
+    out[r * ldo + c0 + j] = (TO)(float)in[i];
+  }
+}
+
+cudaError_t launch_convert_cols(int mode, const double* in, int w, long long rows, void* out, long long ldo,
+                                long long c0, cudaStream_t st) {
+  const long long len = rows * w;
+  if (len <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)std::min<long long>((len + 255) / 256, 148 * 32);
+  if (mode == 1) convert_cols_kernel<float><<<grid, 256, 0, st>>>(in, w, rows, (float*)out, ldo, c0);
+  else convert_cols_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(in, w, rows, (__nv_bfloat16*)out, ldo, c0);
   return cudaGetLastError();
 }
 

@@ -768,11 +768,13 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
     CK(Pinc.alloc(nspin * nn));
     CK(dP.alloc((nspin + 1) * nn));
   }
-  int since_full = -1, builds_inc = 0;
-  auto fock_mixed = [&]() -> int {
-    if (!incremental) return fock(jo);
-    if (since_full < 0 || since_full >= rebuild_every) {
-      RK(fock(jo));
+  int since_full = -1, builds_inc = 0, base_prec = -1;
+  // jb: the options of this build; a change of precision (the switch to the
+  // FP64 refinement) starts from a full build
+  auto fock_inc = [&](const hfg_jk_opts& jb) -> int {
+    if (since_full < 0 || since_full >= rebuild_every || jb.precision != base_prec) {
+      base_prec = jb.precision;
+      RK(fock(jb));
       CK(cudaMemcpyAsync(Jinc.p, J.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
       CK(cudaMemcpyAsync(Kinc.p, K.p, nspin * nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
       CK(cudaMemcpyAsync(Pinc.p, P.p, nspin * nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -792,11 +794,11 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
       dpt = dP.p + 2 * nn;
     }
     if (dmax > 0.0) {
-      hfg_jk_opts ji = jo;
-      double thr = std::max(o->incremental_tol / dmax, jo.schwarz_threshold);
+      hfg_jk_opts ji = jb;
+      double thr = std::max(o->incremental_tol / dmax, jb.schwarz_threshold);
       ji.schwarz_threshold = std::pow(10.0, std::floor(std::log10(thr) + 1e-9));
       RK(jk_device_locked(ctx, &ji, nspin, dpt, dP.p, J.p, K.p));
-      ++buildsmix;
+      if (jb.precision == HFG_MIXED) ++buildsmix; else ++builds64;
       ++builds_inc;
       axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(Jinc.p, J.p, 1.0, 1.0, nn);
       axpby_kernel<<<nblk(nspin * nn), 256, 0, ctx->stream>>>(Kinc.p, K.p, 1.0, 1.0, nspin * nn);
@@ -820,8 +822,10 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   std::vector<int> slot;   // history slot of each stored vector, oldest first
   CK(cudaMemcpyAsync(Pprev.p, P.p, nspin * nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
   for (it = 1; it <= o->max_iter; ++it) {
-    if (refining) RK(fock(jo64));
-    else RK(fock_mixed());
+    // incremental (mixed mode): the mixed phase, then the FP64 refinement
+    // from one full FP64 build
+    if (incremental) RK(fock_inc(refining ? jo64 : jo));
+    else RK(fock(refining ? jo64 : jo));
     if (refining) ++refine_done;
     e_tot = energy() + e_nuc;
     const double de = std::fabs(e_tot - prev_e);
@@ -933,7 +937,8 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
     RK(diag(F.p + sp * nn, C.p + sp * (long long)n * m, P.p + sp * nn, s.evals.p + sp * m, nocc[sp]));
   std::vector<double> epsh((size_t)nspin * m);
   CK(cudaMemcpyAsync(epsh.data(), s.evals.p, nspin * m * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  RK(fock(jo64));
+  if (incremental) RK(fock_inc(jo64));
+  else RK(fock(jo64));
   const double e_el = energy();
   res->energy = e_el + e_nuc;
   res->electronic = e_el;
@@ -1050,8 +1055,17 @@ extern "C" int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts*
     RK(s.gemm(CUBLAS_OP_N, CUBLAS_OP_T, n, n, no, 2.0, Cm, n, Cm, n, 0.0, Pm, n));
     return HFG_OK;
   };
+  // Precision phases: with a tensor-core mode (TF32 / BF16) the Fock matrix
+  // carries rounding noise of the GEMMs, so the SCF first converges loosely
+  // with it (|dE| <= 1e-5 and residual <= 1e-2, or 25 iterations), then
+  // drops the DIIS history and refines with FP64 arithmetic on the stored
+  // factor (at least two FP64 builds) to the requested criteria.  Only the
+  // factor's storage rounding remains in the refined energy.
+  int cur = mma == HFG_DF_FP64 ? HFG_DF_FP64 : mma;
+  int builds64 = 0, builds_low = 0;
   auto fock = [&](const double* Cm) -> int {
-    RK(df_jk_device(df, Cm, no, J.p, K.p, mma));
+    RK(df_jk_device(df, Cm, no, J.p, K.p, cur));
+    if (cur == HFG_DF_FP64) ++builds64; else ++builds_low;
     CK(cudaMemcpyAsync(F.p, s.H.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
     axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(F.p, J.p, 1.0, 1.0, nn);
     axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(F.p, K.p, -0.5, 1.0, nn);
@@ -1079,14 +1093,29 @@ extern "C" int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts*
     axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(s.tmp1.p, P.p, -1.0, 1.0, nn);
     const double dch = s.maxabs(s.tmp1.p, nn);
     if (!std::isfinite(e) || !std::isfinite(resid)) return set_error(ctx, HFG_ERR_SCF, "DF-HF energy/residual became nonfinite");
-    if (o->verbose) fprintf(stderr, "hfg df-scf %3d  E = %.12f  |e| = %.3e  dP = %.3e\n", it, e, resid, dch);
-    if (std::fabs(e - last) <= o->energy_tol && resid <= o->residual_tol && dch <= o->density_tol) {
+    if (o->verbose) fprintf(stderr, "hfg df-scf %3d  E = %.12f  |e| = %.3e  dP = %.3e  %s\n", it, e, resid, dch,
+                           cur == HFG_DF_FP64 ? "fp64" : "tensor");
+    res->energy = e;  // the latest energy, reported if the SCF does not converge
+    res->electronic = e - e_nuc;
+    res->nuclear = e_nuc;
+    if (cur != HFG_DF_FP64 && ((std::fabs(e - last) <= 1e-5 && resid <= 1e-2) || builds_low >= 25)) {
+      res->energy_before_refinement = e;
+      cur = HFG_DF_FP64;
+      count = 0;
+      slot.clear();
+      Bm.clear();
+      last = INFINITY;
+      RK(diag(F.p, C.p, P.p));
+      continue;
+    }
+    const bool enough64 = mma == HFG_DF_FP64 || builds64 >= 2;
+    if (enough64 && std::fabs(e - last) <= o->energy_tol && resid <= o->residual_tol && dch <= o->density_tol) {
       RK(fock(Cn.p));
       const double ef = energy(Pn.p);
       res->energy = ef;
       res->electronic = ef - e_nuc;
       res->nuclear = e_nuc;
-      res->energy_before_refinement = ef;
+      if (mma == HFG_DF_FP64) res->energy_before_refinement = ef;
       converged = true;
       break;
     }
@@ -1137,6 +1166,8 @@ extern "C" int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts*
   res->iterations = it;
   res->converged = converged ? 1 : 0;
   res->n_mo = m;
+  res->fock_builds_fp64 = builds64;
+  res->fock_builds_mixed = builds_low;
   if (P_out) CK(cudaMemcpyAsync(P_out, Pn.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
   if (F_out) CK(cudaMemcpyAsync(F_out, F.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));
   if (J_out) CK(cudaMemcpyAsync(J_out, J.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream));

@@ -42,6 +42,7 @@ struct JobCopy {
 struct hfg_server {
   int device = 0;
   long long budget = 0, in_use = 0;
+  int mixed_min_ao = 256;  // mixed-precision jobs below this size run FP64
   std::chrono::steady_clock::time_point t0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -123,7 +124,14 @@ void worker(hfg_server* s) {
       o.energy_tol = job.spec.energy_tol;
       o.residual_tol = job.spec.residual_tol;
       o.density_tol = job.spec.density_tol;
+      // precision policy: mixed precision pays only on larger jobs (FP32
+      // quartets, then FP64 refinement builds and extra plans); smaller ones
+      // run FP64 with primitive screening at 1e-15 at most
       o.jk = job.spec.jk;
+      if (o.jk.precision == HFG_MIXED && job.n < s->mixed_min_ao) {
+        o.jk.precision = HFG_FP64;
+        o.jk.prim_threshold = std::min(o.jk.prim_threshold, 1e-15);
+      }
       o.refine_iters = 2;
       hfg_scf_result res{};
       rc = hfg_scf(ctx, &o, &res, nullptr, nullptr, nullptr, nullptr);
@@ -200,6 +208,13 @@ int hfg_server_poll(hfg_server* s, hfg_job_result* out, int max, int* n_out, int
   for (int i = 0; i < k; ++i) out[i] = s->done[i];
   s->done.erase(s->done.begin(), s->done.begin() + k);
   *n_out = k;
+  return HFG_OK;
+}
+
+int hfg_server_set_mixed_min_ao(hfg_server* s, int n_ao) {
+  if (!s || n_ao < 0) return HFG_ERR_INVALID_INPUT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->mixed_min_ao = n_ao;
   return HFG_OK;
 }
 

@@ -168,6 +168,7 @@ def load_library():
     L.hfg_server_submit.argtypes = [VP, P(Job)]
     L.hfg_server_poll.argtypes = [VP, P(JobResult), ctypes.c_int, P(ctypes.c_int), ctypes.c_int]
     L.hfg_server_stats.argtypes = [VP, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_longlong)]
+    L.hfg_server_set_mixed_min_ao.argtypes = [VP, ctypes.c_int]
     L.hfg_server_destroy.argtypes = [VP]
     L.hfg_scf.argtypes = [VP, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     _lib = L
@@ -449,13 +450,15 @@ class DFTensor:
 class Server:
     """hfg_server: continuous admission of SCF jobs onto worker slots."""
 
-    def __init__(self, device=0, slots=8, hbm_budget_bytes=64 << 30):
+    def __init__(self, device=0, slots=8, hbm_budget_bytes=64 << 30, mixed_min_ao=None):
         self.lib = load_library()
         h = VP()
         rc = self.lib.hfg_server_create(device, slots, hbm_budget_bytes, ctypes.byref(h))
         if rc != 0:
             raise HfgError(rc, "hfg_server_create failed")
         self.h = h
+        if mixed_min_ao is not None:
+            self.lib.hfg_server_set_mixed_min_ao(h, mixed_min_ao)
 
     def submit(self, basis, charge=0, multiplicity=1, uhf=False, spherical=False, tol=1e-10, max_iter=100,
                jk=None, tag=0):

@@ -322,6 +322,10 @@ int hfg_server_submit(hfg_server* server, const hfg_job* job);
    or nothing is pending or running. */
 int hfg_server_poll(hfg_server* server, hfg_job_result* out, int max, int* n_out, int wait_for_one);
 int hfg_server_stats(hfg_server* server, int* pending, int* running, long long* in_use_bytes);
+/* Jobs submitted with HFG_MIXED J/K options but fewer than n_ao basis
+   functions run FP64 (primitive screening at 1e-15 at most): on small jobs
+   the refinement builds cost more than FP32 saves.  Default 256. */
+int hfg_server_set_mixed_min_ao(hfg_server* server, int n_ao);
 /* Finishes the queued jobs, then stops the workers. */
 int hfg_server_destroy(hfg_server* server);
 

@@ -68,3 +68,36 @@ def test_df_pair_screening_changes_little():
     J0, K0 = DFTensor(ctx, aux).jk(C)
     J1, K1 = DFTensor(ctx, aux, pair_threshold=1e-10).jk(C)
     assert np.max(np.abs(J1 - J0)) < 1e-7 and np.max(np.abs(K1 - K0)) < 1e-7
+
+
+def test_df_chunked_build_matches_single_chunk(monkeypatch):
+    # B built over many narrow column chunks equals the one-chunk build
+    atoms = water_cluster(2)
+    ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
+    aux = CartesianBasis.build(atoms, "def2-universal-jkfit")
+    C = occ_coeffs(ctx.n, 10, 5)
+    for storage, tol in [(HFG_DF_FP64, 1e-11), (HFG_DF_FP32, 1e-5), (HFG_DF_BF16, 2e-2)]:
+        monkeypatch.delenv("HFG_DF_CHUNK_COLS", raising=False)
+        J1, K1 = DFTensor(ctx, aux, storage=storage).jk(C, mma=storage)
+        monkeypatch.setenv("HFG_DF_CHUNK_COLS", "64")
+        d = DFTensor(ctx, aux, storage=storage)
+        assert d.sizes()[2] > 10 * 64  # about 20 chunks
+        J2, K2 = d.jk(C, mma=storage)
+        assert np.max(np.abs(J2 - J1)) < tol and np.max(np.abs(K2 - K1)) < tol, storage
+
+
+@pytest.mark.parametrize("storage,mma,tol", [(HFG_DF_FP32, HFG_DF_FP32, 1e-5), (HFG_DF_FP32, HFG_DF_BF16, 1e-5),
+                                              (HFG_DF_BF16, HFG_DF_BF16, 0.2)])
+def test_df_rhf_tensor_core_phase_then_fp64_refinement(storage, mma, tol):
+    # TF32 / BF16 J/K until loosely converged, then FP64 arithmetic on the
+    # stored factor: converges, and differs from FP64 DF only by the storage
+    # rounding of B (FP32 storage: ~2e-6 Eh of 152 Eh, about 1e-8 relative;
+    # BF16 storage: ~0.11 Eh, 7e-4 relative)
+    atoms = water_cluster(2)
+    ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
+    aux = CartesianBasis.build(atoms, "def2-universal-jkfit")
+    e64 = ctx.scf_df(DFTensor(ctx, aux), spherical=True)
+    r = ctx.scf_df(DFTensor(ctx, aux, storage=storage), mma=mma, spherical=True)
+    assert e64["converged"] and r["converged"]
+    assert r["fock_builds_mixed"] > 0 and r["fock_builds_fp64"] >= 2
+    assert abs(r["energy"] - e64["energy"]) < tol
