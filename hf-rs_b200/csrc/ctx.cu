@@ -466,6 +466,7 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
       const double target = total / ((double)sms * 32 * 8);
       size_t e = 0;
       long long t = 0;
+      L.cost_prefix.assign(1, 0.0);
       while (t < nw_total) {
         while (L.prefix[e + 1] <= t) ++e;
         cstart.push_back(t);
@@ -479,6 +480,7 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
           ++t;
           ++k;
         }
+        L.cost_prefix.push_back(L.cost_prefix.back() + acc);
       }
       cstart.push_back(nw_total);
       if (chunk_entry.empty()) chunk_entry.push_back(0);
@@ -580,7 +582,8 @@ __global__ void fock_kernel(const double* __restrict__ H, const double* __restri
 }
 
 int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs,
-                     double* dJ, double* dK) {
+                     double* dJ, double* dK, int shard, int nshards) {
+  if (nshards < 1 || shard < 0 || shard >= nshards) return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid shard");
   hfg_jk_opts o;
   if (opts) o = *opts; else hfg_jk_opts_default(&o);
   if (nspin < 1 || nspin > 2) return set_error(ctx, HFG_ERR_INVALID_INPUT, "nspin must be 1 or 2");
@@ -626,9 +629,24 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
     a.counter = ctx->d_counters.p + l;
     a.entries = L.d_entries;
     a.prefix = L.d_prefix;
-    a.chunk_entry = L.d_chunk;
-    a.chunk_start = L.d_cstart;
-    a.nchunks = L.nchunks;
+    // shard: steps [c0, c1) with about shard/nshards .. (shard+1)/nshards of
+    // the launch's nominal cost
+    long long c0 = 0, c1 = L.nchunks;
+    if (nshards > 1) {
+      const double tot = L.cost_prefix.back();
+      auto cut = [&](int k) -> long long {
+        if (k <= 0) return 0;
+        if (k >= nshards) return L.nchunks;
+        const double target = tot * (double)k / (double)nshards;
+        return (long long)(std::lower_bound(L.cost_prefix.begin(), L.cost_prefix.end(), target) -
+                           L.cost_prefix.begin());
+      };
+      c0 = std::min(cut(shard), L.nchunks);
+      c1 = std::min(std::max(cut(shard + 1), c0), L.nchunks);
+    }
+    a.chunk_entry = L.d_chunk + c0;
+    a.chunk_start = L.d_cstart + c0;
+    a.nchunks = c1 - c0;
     a.nentries = (int)L.prefix[0];
     a.nwarps = L.prefix[1];
     HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.G, L.fp32, a, ctx->stream));
@@ -832,6 +850,15 @@ int hfg_shell_quartet(hfg_ctx* ctx, int a, int b, int c, int d, double* out) {
           out[((i * ob + j) * oc + k) * od + l] = blk[((I * nb + J) * nc + K) * nd + L];
         }
   return HFG_OK;
+}
+
+int hfg_jk_device_shard(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs,
+                        double* dJ, double* dK, int shard, int nshards) {
+  if (!ctx || !dPt || !dPs || !dJ || !dK) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  AllocScope alloc_scope(ctx->stream);
+  cudaSetDevice(ctx->device);
+  return jk_device_locked(ctx, opts, nspin, dPt, dPs, dJ, dK, shard, nshards);
 }
 
 int hfg_jk_device(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs, double* dJ,

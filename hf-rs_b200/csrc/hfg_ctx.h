@@ -38,6 +38,7 @@ struct Launch {
   int* d_chunk = nullptr;             // entry of the first task of every work-queue step
   long long* d_cstart = nullptr;      // first task of every step (nchunks + 1)
   long long nchunks = 0;
+  std::vector<double> cost_prefix;  // nominal cost of steps [0, c) (nchunks + 1)
 };
 
 struct Plan {
@@ -127,8 +128,10 @@ namespace hfg {
 // Implemented in df.cu: DF J/K from column-major occupied coefficients.
 int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK, int mma);
 // Implemented in ctx.cu, used by scf.cu.
+// shard / nshards: only the shard's cost-balanced range of work-queue steps
+// of every launch (the partial J/K of all shards sum to the full build)
 int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs,
-                     double* dJ, double* dK);
+                     double* dJ, double* dK, int shard = 0, int nshards = 1);
 int set_error(hfg_ctx* ctx, int code, const std::string& msg);
 int build_shell_list(hfg_ctx* ctx, const hfg_basis* b, int lmax);
 void make_pair(const hfg_ctx* ctx, int a, int b, PairInfo& pi, std::vector<PrimPair>& pp, int owner);

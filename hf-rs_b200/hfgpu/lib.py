@@ -150,6 +150,7 @@ def load_library():
     L.hfg_eri_packed_device.argtypes = [VP, ctypes.c_double, VP, ctypes.c_size_t]
     L.hfg_jk.argtypes = [VP, P(JKOptions), ctypes.c_int, DP, DP, DP, DP]
     L.hfg_jk_device.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
+    L.hfg_jk_device_shard.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP, ctypes.c_int, ctypes.c_int]
     L.hfg_jk_device_noalloc.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
     L.hfg_fock_rhf.argtypes = [VP, P(JKOptions), DP, DP, DP]
     L.hfg_fock_uhf.argtypes = [VP, P(JKOptions), DP, DP, DP, DP, DP]
@@ -264,6 +265,12 @@ class Context:
         o = opts or JKOptions.make()
         self._check(self.lib.hfg_jk(self.h, ctypes.byref(o), len(spins), _dp(pt), _dp(ps), _dp(J), _dp(K)))
         return J, K
+
+    def jk_device_shard(self, d_total, d_spin, d_J, d_K, shard, nshards, nspin=1, opts=None):
+        """One cost-balanced shard of the device build (hfg_jk_device_shard)."""
+        o = opts or JKOptions.make()
+        self._check(self.lib.hfg_jk_device_shard(self.h, ctypes.byref(o), nspin, d_total, d_spin, d_J, d_K, shard,
+                                                 nshards))
 
     def jk_device(self, d_total, d_spin, d_J, d_K, nspin=1, opts=None):
         """Device-pointer form (integers); runs on the context stream."""

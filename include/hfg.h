@@ -115,6 +115,18 @@ int hfg_eri_packed_device(hfg_ctx* ctx, double schwarz_threshold, double* d_out,
 int hfg_jk(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* P_total, const double* P_spin,
            double* J, double* K);
 
+/*
+ * One shard of a J/K build for a multi-GPU Fock build (no hf-rs counterpart:
+ * hf-rs parallelises one process with Rayon).  Every launch's work queue is
+ * cut into `nshards` ranges of equal nominal cost and this call runs range
+ * `shard`, so J and K of all shards sum to hfg_jk_device's (J/K are linear in
+ * the integrals).  Device pointers, context stream; each rank of a
+ * multi-GPU build calls it with its own shard and then sums J and K over the
+ * ranks (one all-reduce of (1 + nspin) n^2 doubles).
+ */
+int hfg_jk_device_shard(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* d_P_total,
+                        const double* d_P_spin, double* d_J, double* d_K, int shard, int nshards);
+
 /* As hfg_jk with device pointers, on the context stream, without copies. */
 int hfg_jk_device(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* d_P_total,
                   const double* d_P_spin, double* d_J, double* d_K);

@@ -168,3 +168,31 @@ def test_autotune_picks_fastest_within_energy_budget():
     dE = 0.5 * np.sum(P * (J1 - J0)) - 0.25 * np.sum(P * (K1[0] - K0[0]))
     assert abs(dE - rep["best_energy_error"]) < 1e-10
     assert abs(dE) <= 5e-9
+
+
+@pytest.mark.parametrize("nshards", [2, 3, 5])
+def test_shards_sum_to_the_full_build(nshards):
+    # the multi-GPU decomposition, run shard after shard on one GPU: the
+    # partial J/K of all shards sum to the single build (FP64 and mixed)
+    import torch
+    dev = torch.device("cuda", 0)
+    atoms = water_cluster(4)
+    ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
+    n = ctx.n
+    P = torch.from_numpy(rand_sym(n, 9)).to(dev)
+    J = torch.empty((n, n), dtype=torch.float64, device=dev)
+    K = torch.empty((n, n), dtype=torch.float64, device=dev)
+    for opts in [JKOptions.make(), JKOptions.make(prim=1e-15, mixed=1e-7)]:
+        torch.cuda.synchronize()
+        ctx.jk_device(P.data_ptr(), P.data_ptr(), J.data_ptr(), K.data_ptr(), 1, opts)
+        ctx.jk_device(P.data_ptr(), P.data_ptr(), J.data_ptr(), K.data_ptr(), 1, opts)  # plan made
+        torch.cuda.synchronize()
+        J0, K0 = J.cpu().numpy().copy(), K.cpu().numpy().copy()
+        Js, Ks = np.zeros_like(J0), np.zeros_like(K0)
+        for s in range(nshards):
+            ctx.jk_device_shard(P.data_ptr(), P.data_ptr(), J.data_ptr(), K.data_ptr(), s, nshards, opts=opts)
+            torch.cuda.synchronize()
+            Js += J.cpu().numpy()
+            Ks += K.cpu().numpy()
+        assert np.max(np.abs(Js - J0)) < 1e-11
+        assert np.max(np.abs(Ks - K0)) < 1e-11
