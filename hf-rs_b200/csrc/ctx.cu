@@ -261,7 +261,12 @@ static int build_pairs(hfg_ctx* ctx) {
   dq.release();
   dpb.release();
   for (size_t i = 0; i < gprim.size(); ++i) gprim[i].bound = PB[i];
-  // sort each class by Q descending (ties: hf-rs order), primitives by bound
+  // Sort each class into Schwarz-bound buckets of a factor 4 (descending)
+  // and, within a bucket, by the AO index of its shells: the 32 kets of a
+  // warp then lie close together, so the digestion's density loads and K
+  // atomics along the bra's rows hit few cache lines.  The significant kets
+  // of a bra are whole buckets plus, in the last one, those passing the
+  // exact per-lane test.  Primitives are sorted by bound.
   ctx->h_pairs.clear();
   ctx->h_prims.clear();
   ctx->sorted_Q.clear();
@@ -270,7 +275,23 @@ static int build_pairs(hfg_ctx* ctx) {
   for (auto& c : ctx->classes) {
     std::vector<int> idx(c.count);
     std::iota(idx.begin(), idx.end(), c.first);
-    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return Q[x] > Q[y]; });
+    auto bucket = [&](int x) { return Q[x] > 0.0 ? (int)std::floor(0.5 * std::log2(Q[x])) : -(1 << 20); };
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+      const int bx = bucket(x), by = bucket(y);
+      if (bx != by) return bx > by;
+      if (gp[x].ao_a != gp[y].ao_a) return gp[x].ao_a < gp[y].ao_a;
+      return gp[x].ao_b < gp[y].ao_b;
+    });
+    c.bstart.clear();
+    c.bqmax.clear();
+    for (int k = 0; k < c.count; ++k) {
+      if (k == 0 || bucket(idx[k]) != bucket(idx[k - 1])) {
+        c.bstart.push_back(k);
+        c.bqmax.push_back(0.0);
+      }
+      c.bqmax.back() = std::max(c.bqmax.back(), Q[idx[k]]);
+    }
+    c.bstart.push_back(c.count);
     c.first = (int)ctx->h_pairs.size();
     for (int g : idx) {
       PairInfo pi = gp[g];
@@ -286,6 +307,9 @@ static int build_pairs(hfg_ctx* ctx) {
       ctx->sorted_Q.push_back(Q[g]);
     }
   }
+  HFG_CUDA(ctx, ctx->d_pairQ.alloc(ctx->sorted_Q.size()));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_pairQ.p, ctx->sorted_Q.data(), ctx->sorted_Q.size() * sizeof(double),
+                                cudaMemcpyHostToDevice, ctx->stream));
   HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_pairs.p, ctx->h_pairs.data(), ctx->h_pairs.size() * sizeof(PairInfo),
                                 cudaMemcpyHostToDevice, ctx->stream));
   HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_prims.p, ctx->h_prims.data(), ctx->h_prims.size() * sizeof(PrimPair),
@@ -378,24 +402,20 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
       const double w = wmd_flops(B.la, B.lb, Kc.la, Kc.lb);
       for (int i = B.first; i < B.first + B.count; ++i) {
         const double qi = Q[i];
-        // number of kets with qi * qj > thr (Q sorted descending)
-        int lo = 0, hi = Kc.count;
-        while (lo < hi) {
-          const int mid = (lo + hi) / 2;
-          if (qi * Q[Kc.first + mid] > thr) lo = mid + 1; else hi = mid;
-        }
-        int nsig = lo;
+        // kets in the buckets that can hold qi * qj > thr (whole buckets;
+        // the kernels test each quartet exactly)
+        const int nb = (int)Kc.bqmax.size();
+        int jb = 0;
+        while (jb < nb && qi * Kc.bqmax[jb] > thr) ++jb;
+        int nsig = Kc.bstart[jb];
         if (cb == ck) nsig = std::min(nsig, i - B.first + 1);
         if (nsig <= 0) continue;
         int n64 = nsig;
         if (precision == HFG_MIXED) {
-          lo = 0;
-          hi = nsig;
-          while (lo < hi) {
-            const int mid = (lo + hi) / 2;
-            if (qi * Q[Kc.first + mid] >= mixed) lo = mid + 1; else hi = mid;
-          }
-          n64 = lo;
+          // FP32 only for buckets whose every ket has qi * qj < mixed
+          int jm = 0;
+          while (jm < nb && qi * Kc.bqmax[jm] >= mixed) ++jm;
+          n64 = std::min(nsig, Kc.bstart[jm]);
         }
         const int ranges[2][2] = {{0, n64}, {n64, nsig}};
         for (int r = 0; r < 2; ++r) {
@@ -506,31 +526,37 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     L.entries.shrink_to_fit();
     L.prefix.assign({(long long)ne, nw});
   }
-  if (prim_eps > 0.0) {
-    // exact primitive-quartet counts after primitive screening
+  {
+    // exact shell- and primitive-quartet counts (per-lane Schwarz test and
+    // primitive screening, as the kernels do)
     DevBuf<unsigned long long> cnt;
-    HFG_CUDA(ctx, cnt.alloc(plan->launches.size()));
-    HFG_CUDA(ctx, cudaMemsetAsync(cnt.p, 0, plan->launches.size() * 8, ctx->stream));
-    for (size_t l = 0; l < plan->launches.size(); ++l) {
+    const size_t nl = plan->launches.size();
+    HFG_CUDA(ctx, cnt.alloc(2 * nl));
+    HFG_CUDA(ctx, cudaMemsetAsync(cnt.p, 0, 2 * nl * 8, ctx->stream));
+    for (size_t l = 0; l < nl; ++l) {
       const Launch& L = plan->launches[l];
       HFG_CUDA(ctx, launch_count(L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1], L.G, ctx->d_pairs.p,
-                                 ctx->d_pbound.p, prim_eps, cnt.p + l, ctx->stream));
+                                 ctx->d_pairQ.p, thr, ctx->d_pbound.p, prim_eps, cnt.p + 2 * l, ctx->stream));
     }
-    std::vector<unsigned long long> h(plan->launches.size());
+    std::vector<unsigned long long> h(2 * nl);
     HFG_CUDA(ctx, cudaMemcpyAsync(h.data(), cnt.p, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
     HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     cnt.release();
     st.prim_quartets_fp64 = st.prim_quartets_fp32 = st.wmd_flops_fp64 = st.wmd_flops_fp32 = 0.0;
-    for (size_t l = 0; l < plan->launches.size(); ++l) {
+    st.quartets_fp64 = st.quartets_fp32 = 0.0;
+    for (size_t l = 0; l < nl; ++l) {
       Launch& L = plan->launches[l];
-      L.prims = (double)h[l];
+      L.prims = (double)h[2 * l];
+      L.quartets = (double)h[2 * l + 1];
       const double w = wmd_flops(L.la, L.lb, L.lc, L.ld);
       if (L.fp32) {
-        st.prim_quartets_fp32 += (double)h[l];
-        st.wmd_flops_fp32 += (double)h[l] * w;
+        st.prim_quartets_fp32 += L.prims;
+        st.quartets_fp32 += L.quartets;
+        st.wmd_flops_fp32 += L.prims * w;
       } else {
-        st.prim_quartets_fp64 += (double)h[l];
-        st.wmd_flops_fp64 += (double)h[l] * w;
+        st.prim_quartets_fp64 += L.prims;
+        st.quartets_fp64 += L.quartets;
+        st.wmd_flops_fp64 += L.prims * w;
       }
     }
   }
@@ -602,6 +628,8 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.p, 0, (plan->launches.size() + 1) * 8, ctx->stream));
   JKLaunchArgs a{};
   a.pairs = ctx->d_pairs.p;
+  a.pairQ = ctx->d_pairQ.p;
+  a.thr = o.schwarz_threshold;
   a.rec64 = ctx->d_rec64.p;
   a.rec32 = ctx->d_rec32.p;
   a.pbound = ctx->d_pbound.p;
@@ -688,6 +716,9 @@ hfg_ctx::~hfg_ctx() {
       if (L.d_chunk) cudaFreeAsync(L.d_chunk, L.st);
       if (L.d_cstart) cudaFreeAsync(L.d_cstart, L.st);
     }
+  // every device buffer is released here, before the context's stream is
+  // destroyed (their frees are ordered on it)
+  d_pairQ.release();
   d_pairs.release();
   d_prims.release();
   d_rec64.release();
@@ -909,7 +940,7 @@ static int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len
   for (const Launch& L : plan->launches) {
     if (L.G != 1) return set_error(ctx, HFG_ERR_UNSUPPORTED, "packed tensor: cooperative launch groups");
     HFG_CUDA(ctx, launch_eri_packed(L.la, L.lb, L.lc, L.ld, L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1],
-                                    ctx->d_pairs.p, ctx->d_rec64.p, ctx->d_boys64.p, ctx->d_expt64.p, d_out,
+                                    ctx->d_pairs.p, ctx->d_pairQ.p, thr, ctx->d_rec64.p, ctx->d_boys64.p, ctx->d_expt64.p, d_out,
                                     ctx->stream));
   }
   return HFG_OK;

@@ -25,6 +25,7 @@ template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(128) eri_packed_kernel(const JKEntry* __restrict__ entries,
                                                          const long long* __restrict__ prefix, int nentries,
                                                          long long nwarps, const PairInfo* __restrict__ pairs,
+                                                         const double* __restrict__ pairQ, double thr,
                                                          const PrimRec64* __restrict__ rec,
                                                          const double* __restrict__ boys,
                                                          const double* __restrict__ expt, double* __restrict__ out) {
@@ -40,7 +41,7 @@ __global__ void __launch_bounds__(128) eri_packed_kernel(const JKEntry* __restri
   const int e = find_entry(prefix, nentries, warp);
   const JKEntry ent = entries[e];
   const int kidx = ent.k_lo + (int)(warp - prefix[e]) * 32 + lane;
-  if (kidx >= ent.k_hi) return;
+  if (kidx >= ent.k_hi || !(pairQ[kidx] * pairQ[ent.bra] > thr)) return;
   const PairInfo bra = pairs[ent.bra], ket = pairs[kidx];
   const double ACx = bra.Ax - ket.Ax, ACy = bra.Ay - ket.Ay, ACz = bra.Az - ket.Az;
   double acc[C::NACC];
@@ -81,7 +82,8 @@ __global__ void __launch_bounds__(128) eri_packed_kernel(const JKEntry* __restri
 }
 
 cudaError_t launch_eri_packed(int la, int lb, int lc, int ld, const JKEntry* entries, const long long* prefix,
-                              int nentries, long long nwarps, const PairInfo* pairs, const PrimRec64* rec,
+                              int nentries, long long nwarps, const PairInfo* pairs, const double* pairQ,
+                              double thr, const PrimRec64* rec,
                               const double* boys, const double* expt, double* out, cudaStream_t st) {
   if (nwarps <= 0) return cudaSuccess;
   const int smem = (int)boys_smem_bytes<double>();
@@ -91,7 +93,7 @@ cudaError_t launch_eri_packed(int la, int lb, int lc, int ld, const JKEntry* ent
   if (la == A && lb == B && lc == C && ld == D) {                                                             \
     cudaFuncSetAttribute(eri_packed_kernel<A, B, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);   \
     eri_packed_kernel<A, B, C, D><<<(unsigned)grid, block, smem, st>>>(entries, prefix, nentries, nwarps, pairs, \
-                                                                      rec, boys, expt, out);                  \
+                                                                      pairQ, thr, rec, boys, expt, out);      \
     return cudaGetLastError();                                                                                \
   }
   HFG_CASE(0, 0, 0, 0)

@@ -24,6 +24,11 @@ struct Shell {
 struct PairClass {
   int la, lb, Ka, Kb;
   int first, count;  // range of the sorted global pair table
+  // Schwarz-bound buckets (factor 4, descending) of the class: bucket j holds
+  // pairs [first + bstart[j], first + bstart[j + 1]), ordered by AO index,
+  // with largest bound bqmax[j]
+  std::vector<int> bstart;
+  std::vector<double> bqmax;
 };
 
 struct Launch {
@@ -102,6 +107,7 @@ struct hfg_ctx {
   std::vector<std::pair<int, int>> ref_pairs;  // hf-rs order: (a, b), a >= b
   std::vector<int> ref_to_sorted;             // hf-rs pair index -> sorted pair index
   std::vector<double> sorted_Q;               // Schwarz bound per sorted pair
+  hfg::DevBuf<double> d_pairQ;                // the same on the device (per-lane screening)
   std::vector<hfg::PairInfo> h_pairs;         // sorted pair table
   std::vector<hfg::PrimPair> h_prims;
   std::vector<hfg::PairClass> classes;

@@ -59,6 +59,8 @@ struct JKLaunchArgs {
   long long nchunks;
   long long nwarps;
   const PairInfo* pairs;
+  const double* pairQ;  // Schwarz bound per pair; a lane's quartet counts if Q_bra Q_ket > thr
+  double thr;
   const PrimRec64* rec64;
   const PrimRec32* rec32;
   const float* pbound;  // primitive-pair bounds, sorted descending within each pair

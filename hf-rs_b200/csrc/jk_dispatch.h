@@ -58,12 +58,14 @@ inline int choose_group(int la, int lb, int lc, int ld, long kk) {
 }
 cudaError_t launch_schwarz(int la, int lb, const PairInfo* pairs, const PrimPair* prims, int first, int count,
                            const double* boys, const double* expt, double* out, int prim_mode, cudaStream_t st);
+// out[0] += evaluated primitive quartets, out[1] += evaluated shell quartets
 cudaError_t launch_count(const JKEntry* entries, const long long* prefix, int nentries, long long nwarps, int G,
-                         const PairInfo* pairs, const float* pbound, double eps, unsigned long long* out,
-                         cudaStream_t st);
+                         const PairInfo* pairs, const double* pairQ, double thr, const float* pbound, double eps,
+                         unsigned long long* out, cudaStream_t st);
 cudaError_t fma_peak(int fp32, double* tflops);
 cudaError_t launch_eri_packed(int la, int lb, int lc, int ld, const JKEntry* entries, const long long* prefix,
-                              int nentries, long long nwarps, const PairInfo* pairs, const PrimRec64* rec,
+                              int nentries, long long nwarps, const PairInfo* pairs, const double* pairQ,
+                              double thr, const PrimRec64* rec,
                               const double* boys, const double* expt, double* out, cudaStream_t st);
 cudaError_t launch_quartet(int la, int lb, int lc, int ld, const PairInfo* pairs, const PrimPair* prims,
                            const double* boys, const double* expt, double* out, cudaStream_t st);

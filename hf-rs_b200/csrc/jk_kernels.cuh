@@ -233,7 +233,8 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
       const JKEntry ent = a.entries[e];
       const int grp = lane / G, gl = lane - grp * G;
       const int kidx = ent.k_lo + (int)(warp - a.prefix[e]) * QPW + grp;
-      const bool active = kidx < ent.k_hi;
+      // kets are bucketed by bound: the exact Schwarz test per quartet
+      const bool active = kidx < ent.k_hi && __ldg(a.pairQ + kidx) * __ldg(a.pairQ + ent.bra) > a.thr;
       const PairInfo bra = a.pairs[ent.bra];
       const PairInfo ket = a.pairs[active ? kidx : ent.k_lo];
       // the next task usually continues this entry: start fetching its ket

@@ -13,7 +13,8 @@ namespace hfg {
 
 __global__ void count_kernel(const JKEntry* __restrict__ entries, const long long* __restrict__ prefix, int nentries,
                              long long nwarps, int G, const PairInfo* __restrict__ pairs,
-                             const float* __restrict__ pbound, double eps, unsigned long long* __restrict__ out) {
+                             const double* __restrict__ pairQ, double thr, const float* __restrict__ pbound,
+                             double eps, unsigned long long* __restrict__ out) {
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (warp >= nwarps) return;
   const int lane = threadIdx.x & 31;
@@ -25,8 +26,9 @@ __global__ void count_kernel(const JKEntry* __restrict__ entries, const long lon
   const JKEntry e = entries[lo];
   const int qpw = 32 / G, grp = lane / G, gl = lane - grp * G;
   const int k = e.k_lo + (int)(warp - prefix[lo]) * qpw + grp;
-  unsigned long long c = 0;
-  if (gl == 0 && k < e.k_hi) {
+  unsigned long long c = 0, quartets = 0;
+  if (gl == 0 && k < e.k_hi && pairQ[k] * pairQ[e.bra] > thr) {
+    quartets = 1;
     const PairInfo b = pairs[e.bra], q = pairs[k];
     // the kernels' loop: ket primitive pairs surviving against the largest bra
     // one, then bra primitive pairs while the product stays above eps
@@ -44,17 +46,21 @@ __global__ void count_kernel(const JKEntry* __restrict__ entries, const long lon
       c += (unsigned long long)l;
     }
   }
-  for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+  for (int off = 16; off > 0; off >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, off);
+    quartets += __shfl_xor_sync(0xffffffffu, quartets, off);
+  }
   if (lane == 0 && c) atomicAdd(out, c);
+  if (lane == 0 && quartets) atomicAdd(out + 1, quartets);
 }
 
 cudaError_t launch_count(const JKEntry* entries, const long long* prefix, int nentries, long long nwarps, int G,
-                         const PairInfo* pairs, const float* pbound, double eps, unsigned long long* out,
-                         cudaStream_t st) {
+                         const PairInfo* pairs, const double* pairQ, double thr, const float* pbound, double eps,
+                         unsigned long long* out, cudaStream_t st) {
   const long long threads = nwarps * 32;
   if (threads == 0) return cudaSuccess;
-  count_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(entries, prefix, nentries, nwarps, G, pairs, pbound,
-                                                                   eps, out);
+  count_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(entries, prefix, nentries, nwarps, G, pairs, pairQ,
+                                                                   thr, pbound, eps, out);
   return cudaGetLastError();
 }
 
