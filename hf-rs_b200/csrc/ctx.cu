@@ -622,10 +622,26 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   const size_t nn = (size_t)ctx->n * ctx->n;
   HFG_CUDA(ctx, ctx->d_Jacc.alloc(nn));
   HFG_CUDA(ctx, ctx->d_Kacc.alloc(2 * nn));
-  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Jacc.p, 0, nn * sizeof(double), ctx->stream));
-  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Kacc.p, 0, nspin * nn * sizeof(double), ctx->stream));
   HFG_CUDA(ctx, ctx->d_counters.alloc(plan->launches.size() + 1));
-  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.p, 0, (plan->launches.size() + 1) * 8, ctx->stream));
+  // HFG_PROFILE=1: per-launch device time (CUDA events) on stderr
+  static const bool profile = getenv("HFG_PROFILE") && getenv("HFG_PROFILE")[0] == '1';
+  // The build is a fixed sequence (clears, one launch per class, two
+  // symmetrisations) whose arguments depend only on the plan and the
+  // buffers.  A sequence seen for the second time is captured into a CUDA
+  // graph and replayed from then on (an SCF reuses its buffers every
+  // iteration); the first build of a sequence always runs eagerly, so the
+  // kernels' one-time attribute and occupancy set-up happens outside any
+  // capture.  Shards and profiled builds run eagerly.
+  const bool graphs_on = ctx->use_graphs && nshards == 1 && !profile;
+  const hfg_ctx::GraphKey key{plan, nspin, dPt, dPs, dJ, dK, ctx->d_Jacc.p, ctx->d_Kacc.p, ctx->d_counters.p};
+  if (graphs_on) {
+    auto it = ctx->graphs.find(key);
+    if (it != ctx->graphs.end()) {
+      HFG_CUDA(ctx, cudaGraphLaunch(it->second, ctx->stream));
+      ctx->last = plan->stats;
+      return HFG_OK;
+    }
+  }
   JKLaunchArgs a{};
   a.pairs = ctx->d_pairs.p;
   a.pairQ = ctx->d_pairQ.p;
@@ -644,8 +660,10 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   a.n = ctx->n;
   a.nspin = nspin;
   a.prim_eps = o.prim_threshold;
-  // HFG_PROFILE=1: per-launch device time (CUDA events) on stderr
-  static const bool profile = getenv("HFG_PROFILE") && getenv("HFG_PROFILE")[0] == '1';
+  auto enqueue = [&]() -> int {
+  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Jacc.p, 0, nn * sizeof(double), ctx->stream));
+  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Kacc.p, 0, nspin * nn * sizeof(double), ctx->stream));
+  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.p, 0, (plan->launches.size() + 1) * 8, ctx->stream));
   std::vector<cudaEvent_t> ev;
   if (profile) {
     ev.resize(plan->launches.size() + 1);
@@ -702,6 +720,34 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   HFG_CUDA(ctx, (symmetrize_kernel<<<(unsigned)((nspin * nn + blk - 1) / blk), blk, 0, ctx->stream>>>(
                      ctx->d_Kacc.p, dK, ctx->n, nspin),
                  cudaGetLastError()));
+  return HFG_OK;
+  };
+  if (graphs_on && !ctx->graph_failed.count(key)) {
+    if (ctx->graph_seen.count(key)) {
+      // second build of this sequence: capture it, then launch the graph
+      cudaGraph_t g = nullptr;
+      cudaGraphExec_t ge = nullptr;
+      if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int erc = enqueue();
+        const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &g);
+        if (erc == HFG_OK && ec == cudaSuccess && g && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess)
+          ctx->graphs.emplace(key, ge);
+        if (g) cudaGraphDestroy(g);
+      }
+      cudaGetLastError();  // a failed capture leaves an error; the build then runs eagerly
+      auto it = ctx->graphs.find(key);
+      if (it != ctx->graphs.end()) {
+        HFG_CUDA(ctx, cudaGraphLaunch(it->second, ctx->stream));
+        ctx->last = plan->stats;
+        return HFG_OK;
+      }
+      ctx->graph_failed.insert(key);
+    } else {
+      ctx->graph_seen.insert(key);
+    }
+  }
+  rc = enqueue();
+  if (rc != HFG_OK) return rc;
   ctx->last = plan->stats;
   return HFG_OK;
 }
@@ -716,6 +762,7 @@ hfg_ctx::~hfg_ctx() {
       if (L.d_chunk) cudaFreeAsync(L.d_chunk, L.st);
       if (L.d_cstart) cudaFreeAsync(L.d_cstart, L.st);
     }
+  for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
   // every device buffer is released here, before the context's stream is
   // destroyed (their frees are ordered on it)
   d_pairQ.release();
@@ -754,6 +801,8 @@ int hfg_ctx_create(const hfg_basis* basis, int device, void* stream, hfg_ctx** o
   *out = nullptr;
   auto ctx = std::make_unique<hfg_ctx>();
   ctx->device = device;
+  // HFG_NO_GRAPHS=1: every J/K build launches eagerly
+  ctx->use_graphs = !(getenv("HFG_NO_GRAPHS") && getenv("HFG_NO_GRAPHS")[0] == '1');
   int rc = cuda_check(ctx.get(), cudaSetDevice(device), "cudaSetDevice");
   if (rc == HFG_OK) {
     if (stream) ctx->stream = (cudaStream_t)stream;

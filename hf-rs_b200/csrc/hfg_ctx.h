@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <set>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -106,6 +108,12 @@ struct hfg_ctx {
   std::vector<double> exps, coefs;
   std::vector<std::pair<int, int>> ref_pairs;  // hf-rs order: (a, b), a >= b
   std::vector<int> ref_to_sorted;             // hf-rs pair index -> sorted pair index
+  // J/K builds replayed as CUDA graphs, keyed by plan and buffers
+  using GraphKey = std::tuple<const void*, int, const void*, const void*, const void*, const void*, const void*,
+                              const void*, const void*>;
+  bool use_graphs = true;
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  std::set<GraphKey> graph_seen, graph_failed;
   std::vector<double> sorted_Q;               // Schwarz bound per sorted pair
   hfg::DevBuf<double> d_pairQ;                // the same on the device (per-lane screening)
   std::vector<hfg::PairInfo> h_pairs;         // sorted pair table

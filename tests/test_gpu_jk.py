@@ -196,3 +196,30 @@ def test_shards_sum_to_the_full_build(nshards):
             Ks += K.cpu().numpy()
         assert np.max(np.abs(Js - J0)) < 1e-11
         assert np.max(np.abs(Ks - K0)) < 1e-11
+
+
+def test_graph_replayed_builds_match_eager(monkeypatch):
+    # the same buffers, new densities each call: build 1 eager, build 2
+    # captured, builds 3-4 replayed; each equals an eager-only context
+    import torch
+    dev = torch.device("cuda", 0)
+    atoms = water_cluster(3)
+    basis = CartesianBasis.build(atoms, "cc-pvdz")
+    monkeypatch.delenv("HFG_NO_GRAPHS", raising=False)
+    ctx = Context(basis)
+    monkeypatch.setenv("HFG_NO_GRAPHS", "1")
+    eager = Context(basis)
+    n = ctx.n
+    P = torch.empty((n, n), dtype=torch.float64, device=dev)
+    J = torch.empty((n, n), dtype=torch.float64, device=dev)
+    K = torch.empty((n, n), dtype=torch.float64, device=dev)
+    for opts in [JKOptions.make(), JKOptions.make(prim=1e-15, mixed=1e-7)]:
+        for call in range(4):
+            Ph = rand_sym(n, 20 + call)
+            P.copy_(torch.from_numpy(Ph))
+            torch.cuda.synchronize()
+            ctx.jk_device(P.data_ptr(), P.data_ptr(), J.data_ptr(), K.data_ptr(), 1, opts)
+            torch.cuda.synchronize()
+            Jg, Kg = J.cpu().numpy().copy(), K.cpu().numpy().copy()
+            Je, Ke = eager.jk(Ph, opts=opts)
+            assert np.max(np.abs(Jg - Je)) < 1e-12 and np.max(np.abs(Kg - Ke[0])) < 1e-12, call
