@@ -1072,7 +1072,22 @@ extern "C" int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts*
     return HFG_OK;
   };
   auto energy = [&](const double* Pm) { return 0.5 * (s.dot(Pm, s.H.p, nn) + s.dot(Pm, F.p, nn)) + e_nuc; };
-  RK(diag(s.H.p, C.p, P.p));
+  if (o->guess == 0) {
+    // SAD start (an option: run_factorized_rhf itself starts from the core
+    // Hamiltonian): one FP64 four-centre build of the SAD density, whose
+    // Fock matrix gives the first orbitals
+    RK(sad_guess(ctx, o, s, electrons, Pn.p));
+    hfg_jk_opts j64;
+    hfg_jk_opts_default(&j64);
+    j64.prim_threshold = 1e-15;
+    RK(jk_device_locked(ctx, &j64, 1, Pn.p, Pn.p, J.p, K.p));
+    CK(cudaMemcpyAsync(F.p, s.H.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(F.p, J.p, 1.0, 1.0, nn);
+    axpby_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(F.p, K.p, -0.5, 1.0, nn);
+    RK(diag(F.p, C.p, P.p));
+  } else {
+    RK(diag(s.H.p, C.p, P.p));
+  }
   double last = INFINITY;
   bool converged = false;
   int it = 0, count = 0;

@@ -355,10 +355,13 @@ class Context:
         o.verbose = int(verbose)
         return o
 
-    def scf_df(self, df, mma=0, charge=0, spherical=False, tol=(1e-12, 1e-10, 1e-10), max_iter=100, verbose=False):
-        """DF-RHF (hfg_scf_df) with a DFTensor built on this context."""
+    def scf_df(self, df, mma=0, charge=0, spherical=False, tol=(1e-12, 1e-10, 1e-10), max_iter=100, verbose=False,
+               guess="core"):
+        """DF-RHF (hfg_scf_df) with a DFTensor built on this context; guess
+        "core" as run_factorized_rhf, or "sad"."""
         keep = []
         o = self._scf_opts(charge, 1, False, spherical, tol, max_iter, None, 0, verbose, keep)
+        o.guess = 0 if guess == "sad" else 1
         n = self.n
         P, F, J, K = (np.zeros((n, n)) for _ in range(4))
         r = SCFResult()

@@ -289,10 +289,14 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* opts, hfg_scf_result* result, doub
 /*
  * Stands in for run_df_hf_with_aux / run_factorized_rhf
  * (src/hf_variants/ri_df_hf.rs:122-263): DF-RHF with the DF tensor `df`
- * built on this context, K GEMMs in `mma` precision.  Uses the nuclei,
- * charge, AO space, iteration limit, tolerances and DIIS size of `opts`.
- * Optional outputs (row-major n x n, NULL to skip): P, F, J, K at
- * convergence.
+ * built on this context.  Uses the nuclei, charge, AO space, iteration
+ * limit, tolerances and DIIS size of `opts`, and its guess: 1 = the core
+ * Hamiltonian, as run_factorized_rhf; 0 = orbitals of the Fock matrix of
+ * the SAD density (one FP64 four-centre build).  `mma` HFG_DF_FP32 (TF32)
+ * or HFG_DF_BF16 runs tensor-core J/K until loosely converged, then FP64
+ * arithmetic on the stored factor to the tolerances; HFG_DF_FP64 runs FP64
+ * throughout.  Optional outputs (row-major n x n, NULL to skip): P, F, J, K
+ * at convergence.
  */
 int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts* opts, hfg_scf_result* result, double* P,
                double* F, double* J, double* K);

@@ -101,3 +101,17 @@ def test_df_rhf_tensor_core_phase_then_fp64_refinement(storage, mma, tol):
     assert e64["converged"] and r["converged"]
     assert r["fock_builds_mixed"] > 0 and r["fock_builds_fp64"] >= 2
     assert abs(r["energy"] - e64["energy"]) < tol
+
+
+def test_df_rhf_sad_start_reaches_the_same_energy():
+    # the SAD start (an option; hf-rs's DF driver starts from the core
+    # Hamiltonian) converges to the same DF-RHF solution in fewer iterations
+    atoms = water_cluster(3)
+    ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
+    aux = CartesianBasis.build(atoms, "def2-universal-jkfit")
+    df = DFTensor(ctx, aux)
+    rc = ctx.scf_df(df, spherical=True)
+    rs = ctx.scf_df(df, spherical=True, guess="sad")
+    assert rc["converged"] and rs["converged"]
+    assert abs(rc["energy"] - rs["energy"]) < 1e-9
+    assert rs["iterations"] < rc["iterations"]
