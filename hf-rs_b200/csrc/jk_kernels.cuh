@@ -155,23 +155,26 @@ __device__ __forceinline__ void digest(const DT* __restrict__ w, const PairInfo&
 }
 
 // Resident blocks per SM that the register allocation of class
-// (LA LB|LC LD) is tuned for (measured on (H2O)64 cc-pVDZ: the light FP32
-// classes gain from 3-4 blocks, the others spill and lose).  The
-// HFG_JK_MIN_BLOCKS_F64 / _F32 macros override the table for tuning builds.
+// (LA LB|LC LD) is tuned for (measured on (H2O)64 cc-pVDZ): the light FP32
+// classes gain from 3-4 blocks; classes whose contracted accumulators do not
+// fit in 128 registers (FP64 with L >= 4, FP32 with L >= 5 and (pp|pp)) run
+// one block with up to 255 registers, since their spills cost more than the
+// lost occupancy.  The HFG_JK_MIN_BLOCKS_F64 / _F32 macros override the
+// table for tuning builds.
 template <int LA, int LB, int LC, int LD, typename T> struct MinBlocks {
   static constexpr int code = LA * 1000 + LB * 100 + LC * 10 + LD;
   static constexpr int L = LA + LB + LC + LD;
 #ifdef HFG_JK_MIN_BLOCKS_F64
   static constexpr int f64 = HFG_JK_MIN_BLOCKS_F64;
 #else
-  static constexpr int f64 = L >= 5 ? 1 : 2;
+  static constexpr int f64 = L >= 4 ? 1 : 2;
 #endif
 #ifdef HFG_JK_MIN_BLOCKS_F32
   static constexpr int f32 = HFG_JK_MIN_BLOCKS_F32;
 #else
   static constexpr int f32 = (code == 0 || code == 1000 || code == 1010)   ? 4
                              : (code == 1100 || code == 2000 || code == 2100) ? 3
-                             : L >= 6                                         ? 1
+                             : (L >= 5 || code == 1111)                       ? 1
                                                                               : 2;
 #endif
   static constexpr int value = sizeof(T) == 4 ? f32 : f64;
