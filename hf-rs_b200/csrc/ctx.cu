@@ -526,9 +526,24 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     L.entries.shrink_to_fit();
     L.prefix.assign({(long long)ne, nw});
   }
+  plan->thr = thr;
+  plan->prim_eps = prim_eps;
+  st.launches = (int)plan->launches.size();
+  plan->stats = st;
+  out = plan.get();
+  ctx->plans[key] = std::move(plan);
+  return HFG_OK;
+}
+
+// Exact shell- and primitive-quartet counts of a plan (the per-lane Schwarz
+// test and primitive screening of the kernels): the work unit of the
+// roofline.  Made on the first stats request only, since an SCF builds
+// plans it never reports on.
+static int count_plan(hfg_ctx* ctx, Plan* plan) {
+  if (plan->counted) return HFG_OK;
+  const double thr = plan->thr, prim_eps = plan->prim_eps;
+  hfg_jk_stats& st = plan->stats;
   {
-    // exact shell- and primitive-quartet counts (per-lane Schwarz test and
-    // primitive screening, as the kernels do)
     DevBuf<unsigned long long> cnt;
     const size_t nl = plan->launches.size();
     HFG_CUDA(ctx, cnt.alloc(2 * nl));
@@ -560,10 +575,7 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
       }
     }
   }
-  st.launches = (int)plan->launches.size();
-  plan->stats = st;
-  out = plan.get();
-  ctx->plans[key] = std::move(plan);
+  plan->counted = true;
   return HFG_OK;
 }
 
@@ -639,6 +651,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
     if (it != ctx->graphs.end()) {
       HFG_CUDA(ctx, cudaGraphLaunch(it->second, ctx->stream));
       ctx->last = plan->stats;
+      ctx->last_plan = plan;
       return HFG_OK;
     }
   }
@@ -666,6 +679,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.p, 0, (plan->launches.size() + 1) * 8, ctx->stream));
   std::vector<cudaEvent_t> ev;
   if (profile) {
+    HFG_CUDA(ctx, count_plan(ctx, plan) == HFG_OK ? cudaSuccess : cudaErrorUnknown);
     ev.resize(plan->launches.size() + 1);
     for (auto& x : ev) cudaEventCreate(&x);
     cudaEventRecord(ev[0], ctx->stream);
@@ -739,6 +753,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
       if (it != ctx->graphs.end()) {
         HFG_CUDA(ctx, cudaGraphLaunch(it->second, ctx->stream));
         ctx->last = plan->stats;
+        ctx->last_plan = plan;
         return HFG_OK;
       }
       ctx->graph_failed.insert(key);
@@ -749,6 +764,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   rc = enqueue();
   if (rc != HFG_OK) return rc;
   ctx->last = plan->stats;
+  ctx->last_plan = plan;
   return HFG_OK;
 }
 
@@ -1197,9 +1213,19 @@ int hfg_fma_peak(int device, int fp32, double* tflops) {
   return fma_peak(fp32, tflops) == cudaSuccess ? HFG_OK : HFG_ERR_CUDA;
 }
 
-int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* st) {
-  if (!ctx || !st) return HFG_ERR_INVALID_INPUT;
-  *st = ctx->last;
+int hfg_jk_last_stats(const hfg_ctx* cctx, hfg_jk_stats* st) {
+  if (!cctx || !st) return HFG_ERR_INVALID_INPUT;
+  hfg_ctx* ctx = const_cast<hfg_ctx*>(cctx);  // the exact counts are made on first request
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->last_plan) {
+    *st = ctx->last;
+    return HFG_OK;
+  }
+  AllocScope alloc_scope(ctx->stream);
+  cudaSetDevice(ctx->device);
+  const int rc = count_plan(ctx, ctx->last_plan);
+  if (rc != HFG_OK) return rc;
+  *st = ctx->last_plan->stats;
   return HFG_OK;
 }
 

@@ -50,7 +50,9 @@ struct Launch {
 
 struct Plan {
   std::vector<Launch> launches;
-  hfg_jk_stats stats{};
+  hfg_jk_stats stats{};  // nominal counts until `counted`
+  double thr = 0.0, prim_eps = 0.0;
+  bool counted = false;  // exact shell/primitive-quartet counts made (on the first stats request)
 };
 
 // Stream on which DevBuf allocations of the current host thread are made
@@ -112,6 +114,7 @@ struct hfg_ctx {
   using GraphKey = std::tuple<const void*, int, const void*, const void*, const void*, const void*, const void*,
                               const void*, const void*>;
   bool use_graphs = true;
+  hfg::Plan* last_plan = nullptr;  // plan of the last J/K build (for hfg_jk_last_stats)
   std::map<GraphKey, cudaGraphExec_t> graphs;
   std::set<GraphKey> graph_seen, graph_failed;
   std::vector<double> sorted_Q;               // Schwarz bound per sorted pair

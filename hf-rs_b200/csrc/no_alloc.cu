@@ -135,5 +135,6 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
   rc = hfg::cuda_check(ctx, cudaGetLastError(), "symmetrize");
   if (rc != HFG_OK) return rc;
   ctx->last = plan.stats;
+  ctx->last_plan = it->second.get();
   return HFG_OK;
 }
