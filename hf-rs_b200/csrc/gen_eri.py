@@ -218,9 +218,9 @@ def class_list(lmax):
     return out
 
 
-def main():
-    lmax = int(sys.argv[1]) if len(sys.argv) > 1 else 2
-    here = os.path.dirname(os.path.abspath(__file__))
+def render(lmax):
+    """The text of eri_gen.cuh for classes up to lmax, and per-class counts
+    of recursion temporaries."""
     parts = ["// Generated by gen_eri.py -- do not edit.  Obara-Saika VRR + HRR per class.",
              "#pragma once",
              "namespace hfg {",
@@ -233,8 +233,15 @@ def main():
         stats.append((la, lb, lc, ld, nv, nh))
     parts.append("#undef T")
     parts.append("}  // namespace hfg")
+    return "\n".join(parts) + "\n", stats
+
+
+def main():
+    lmax = int(sys.argv[1]) if len(sys.argv) > 1 else 2
+    here = os.path.dirname(os.path.abspath(__file__))
+    text, stats = render(lmax)
     with open(os.path.join(here, "eri_gen.cuh"), "w") as f:
-        f.write("\n".join(parts) + "\n")
+        f.write(text)
     for s in stats:
         print("class (%d%d|%d%d): %d vrr temps, %d hrr temps" % s)
 

@@ -31,3 +31,24 @@ def test_convergence_from_tol_matches_the_c_defaults():
     L.load_library().hfg_scf_opts_default(ctypes.byref(o))
     assert L.convergence_from_tol(1e-10) == (o.energy_tol, o.residual_tol, o.density_tol)
     assert o.incremental_tol == 1e-12 and o.rebuild_every == 8 and o.refine_iters == 2 and o.diis_size == 8
+
+
+def test_generated_recursions_match_the_generator():
+    # eri_gen.cuh is the output of gen_eri.py for s, p, d (the Makefile
+    # regenerates it when the generator changes); the committed file must be
+    # exactly what the generator produces
+    import importlib.util
+    import os
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "hf-rs_b200", "csrc")
+    spec = importlib.util.spec_from_file_location("gen_eri", os.path.join(csrc, "gen_eri.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    text, stats = gen.render(2)
+    assert text == open(os.path.join(csrc, "eri_gen.cuh")).read()
+    # every four-centre class the J/K kernels are built for is generated
+    classes = {s[:4] for s in stats}
+    for la in range(3):
+        for lb in range(la + 1):
+            for lc in range(3):
+                for ld in range(lc + 1):
+                    assert (la, lb, lc, ld) in classes
