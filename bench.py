@@ -9,8 +9,9 @@ accumulation) with the density resident in HBM; the same builds in plain
 FP64 are reported beside it.  `e2e` is the same build through the C ABI
 with host buffers (hfg_jk): density host->device, J and K device->host.
 
-Under torchrun each rank builds its own replica (weak scaling, no data-path
-collective); the step time is the maximum over ranks.
+Under torchrun the N ranks share one Fock build (strong scaling): each rank
+runs a cost-balanced shard of every launch's work queue and one NCCL
+all-reduce sums J and K; the step time is the maximum over ranks.
 
 --impl reference times the CPU restatement of hf-rs's path (the oracle:
 the same screened shell quartets, McMurchie-Davidson integrals, contract_jk
@@ -51,7 +52,11 @@ def parse():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-jobs", type=int, default=24)
     ap.add_argument("--serve-max-waters", type=int, default=16)
-    ap.add_argument("--df-waters", type=int, default=0, help="also time DF J/K on (H2O)_n (0: skip)")
+    ap.add_argument("--df-waters", type=int, default=32, help="also time DF J/K on (H2O)_n (0: skip)")
+    ap.add_argument("--scf-waters", type=int, default=-1,
+                    help="full SCF in FP64 and in the mixed form on (H2O)_n (-1: --waters, 0: skip)")
+    ap.add_argument("--jk-only", action="store_true",
+                    help="only the mixed builds (fixed thresholds, no autotuning, no other legs): for profilers")
     return ap.parse_args()
 
 
@@ -235,7 +240,7 @@ def run_reference(args):
             rows = nrows
     v = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload(args.waters, 25 * args.waters) + ", CPU restatement of hf-rs (McMurchie-Davidson, contract_jk)",
                        "parallelism": "openmp-%d" % threads},
@@ -290,6 +295,16 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     torch.cuda.synchronize()
+    if args.jk_only:
+        # profiler runs: the mixed builds alone, with the thresholds the
+        # autotuner picks on this workload
+        opt = JKOptions.make(schwarz=SCHWARZ, prim=1e-13, mixed=1e-6)
+        for _ in range(args.warmup + args.steps):
+            ctx.jk_device(P.data_ptr(), P.data_ptr(), J.data_ptr(), K.data_ptr(), 1, opt)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"jk_only": True, "waters": args.waters, "builds": args.warmup + args.steps}))
+        return
     # mixed form chosen by the autotuner (FP32 threshold 1e-9..1e-6, primitive
     # threshold 1e-15..1e-13, build energy error within 5e-9 Eh of the plain
     # FP64 build); untimed
@@ -429,6 +444,10 @@ def run_ours(args):
     dfres = None
     if world == 1 and args.df_waters > 0:
         dfres = measure_df(args, torch)
+    scfres = None
+    scf_waters = args.waters if args.scf_waters < 0 else args.scf_waters
+    if world == 1 and scf_waters > 0:
+        scfres = measure_scf(scf_waters, ctx if scf_waters == args.waters else None, opt_mixed)
     mt, pt = opt_mixed.mixed_threshold, opt_mixed.prim_threshold
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_mixed / args.steps, "higher_is_better": True,
@@ -449,10 +468,23 @@ def run_ours(args):
             "autotune": {"chosen": {"fp32_threshold": mt, "prim_threshold": pt}, "budget_eh": TUNE_BUDGET,
                          "candidates": tune["candidates"]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck, "serving": serving, "df": dfres,
+            "scf": scfres,
             # per build: the plan's J/K launches plus two symmetrisation kernels;
             # timed: K mixed, K FP64, K plain FP64 and K end-to-end mixed builds
             "gpu_launches": args.steps * (stats_mixed["launches"] + 2) * (1 if e2e is None else 2)
             + args.steps * (stats_fp64["launches"] + 2) + args.steps * (stats_plain["launches"] + 2)}
+    # the figures a reader needs first, last on the line (a log tail keeps them)
+    line["summary"] = {
+        "mixed_ms": round(tot_mixed / args.steps, 2), "fp64_ms": round(tot_fp64 / args.steps, 2),
+        "fp64_plain_ms": round(tot_plain / args.steps, 2),
+        "mixed_over_fp64_plain": round(value / value_plain, 3), "mixed_over_fp64": round(value / value_fp64, 3),
+        "roofline_frac": round(pipe_frac, 4), "e2e_builds_per_s": None if e2e is None else round(e2e["value"], 4),
+        "serving_jobs_per_s_ratio": None if serving is None else round(serving["jobs_per_s_ratio"], 3),
+        "serving_p50_p99_s": None if serving is None else [round(serving["served_mixed_8_slots"]["p50_s"], 3),
+                                                           round(serving["served_mixed_8_slots"]["p99_s"], 3)],
+        "scf_mixed_minus_fp64_eh": None if scfres is None else scfres["mixed_minus_fp64_eh"],
+        "scf_before_refinement_minus_fp64_eh": None if scfres is None else scfres["before_refinement_minus_fp64_eh"],
+        "df_k_tflops": None if dfres is None else dfres.get("k_tflops_best")}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -476,6 +508,39 @@ def measure_serving(args):
     return {"sample": "%d jobs, waters 1..%d, STO-3G/6-31G*/cc-pVDZ, 10%% UHF" % (len(jobs), args.serve_max_waters),
             "sequential_fp64": a, "served_mixed_8_slots": b, "jobs_per_s_ratio": b["jobs_per_s"] / a["jobs_per_s"],
             "max_abs_dE_served_vs_sequential": de}
+
+
+def measure_scf(waters, ctx, opt_mixed):
+    """Full SCF of (H2O)_n cc-pVDZ (spherical AO space, tol 1e-10, SAD start,
+    CDIIS): FP64 builds with primitive screening 1e-15, and the mixed form
+    (incremental builds, FP64 refinement of at least two builds).  Reports
+    both energies, the mixed energy's error and the error before refinement,
+    iterations and wall times (basis to converged energy)."""
+    from hfgpu import CartesianBasis, Context, JKOptions
+    from hfgpu.clusters import water_cluster
+    own = ctx is None
+    if own:
+        ctx = Context(CartesianBasis.build(water_cluster(waters), "cc-pvdz"))
+    out = {"waters": waters, "n_ao": ctx.n, "tol": 1e-10}
+    t0 = time.time()
+    r64 = ctx.scf(spherical=True, tol=1e-10, jk=JKOptions.make(schwarz=SCHWARZ, prim=PRIM), want=())
+    t64 = time.time() - t0
+    t0 = time.time()
+    rmx = ctx.scf(spherical=True, tol=1e-10, jk=opt_mixed, want=())
+    tmx = time.time() - t0
+    out["fp64"] = {"energy": r64["energy"], "iterations": r64["iterations"], "converged": bool(r64["converged"]),
+                   "wall_s": t64, "builds": r64["fock_builds_fp64"]}
+    out["mixed"] = {"energy": rmx["energy"], "energy_before_refinement": rmx["energy_before_refinement"],
+                    "iterations": rmx["iterations"], "converged": bool(rmx["converged"]), "wall_s": tmx,
+                    "builds_mixed": rmx["fock_builds_mixed"], "builds_fp64": rmx["fock_builds_fp64"],
+                    "builds_incremental": rmx["fock_builds_incremental"],
+                    "fp32_threshold": opt_mixed.mixed_threshold, "prim_threshold": opt_mixed.prim_threshold}
+    out["mixed_minus_fp64_eh"] = rmx["energy"] - r64["energy"]
+    out["before_refinement_minus_fp64_eh"] = rmx["energy_before_refinement"] - r64["energy"]
+    out["speedup_wall"] = t64 / tmx
+    if own:
+        ctx.close()
+    return out
 
 
 def measure_df(args, torch):
@@ -510,6 +575,7 @@ def measure_df(args, torch):
                      "max_abs_dJ_vs_fp64": float(np.max(np.abs(J - ref[0]))),
                      "max_abs_dK_vs_fp64": float(np.max(np.abs(K - ref[1])))}
         df.close()
+    out["k_tflops_best"] = max(out[k]["k_gemm_tflops"] for k in ("tf32", "bf16"))
     return out
 
 

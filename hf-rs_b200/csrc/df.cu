@@ -51,6 +51,61 @@ struct hfg_df {
 
 namespace {
 
+// The auxiliary basis as unit-paired "pairs" on the device, grouped by
+// angular momentum (hf-rs's constant() partner, src/df.rs:30-41).
+struct AuxSet {
+  hfg_ctx shells;
+  DevBuf<PairInfo> dup;
+  DevBuf<PrimPair> dupr;
+  std::map<int, std::vector<int>> by_l;
+  std::map<int, DevBuf<int>> idx;
+};
+
+int make_aux_set(hfg_ctx* ctx, const hfg_basis* aux, AuxSet& ax) {
+  cudaStream_t st = ctx->stream;
+  int rc = build_shell_list(&ax.shells, aux, 4);
+  if (rc != HFG_OK) return set_error(ctx, rc, "auxiliary basis: " + ax.shells.err);
+  std::vector<PairInfo> upairs(ax.shells.shells.size());
+  std::vector<PrimPair> uprims;
+  for (size_t s = 0; s < ax.shells.shells.size(); ++s) {
+    const Shell& sh = ax.shells.shells[s];
+    PairInfo& pi = upairs[s];
+    pi = PairInfo{};
+    pi.Ax = sh.c[0];
+    pi.Ay = sh.c[1];
+    pi.Az = sh.c[2];
+    pi.ao_a = sh.ao;
+    pi.pp_off = (int)uprims.size();
+    pi.npp = sh.K;
+    for (int q = 0; q < sh.K; ++q) {
+      PrimPair p{};
+      p.p = ax.shells.exps[sh.prim_off + q];
+      p.inv_p = 1.0 / p.p;
+      p.kp = ax.shells.coefs[sh.prim_off + q] * p.inv_p;  // unit partner: coefficient 1, exp(0) = 1
+      uprims.push_back(p);
+    }
+  }
+  rc = cuda_check(ctx, ax.dup.alloc(upairs.size()), "alloc");
+  if (rc == HFG_OK) rc = cuda_check(ctx, ax.dupr.alloc(uprims.size()), "alloc");
+  if (rc == HFG_OK)
+    rc = cuda_check(ctx, cudaMemcpyAsync(ax.dup.p, upairs.data(), upairs.size() * sizeof(PairInfo),
+                                         cudaMemcpyHostToDevice, st), "copy");
+  if (rc == HFG_OK)
+    rc = cuda_check(ctx, cudaMemcpyAsync(ax.dupr.p, uprims.data(), uprims.size() * sizeof(PrimPair),
+                                         cudaMemcpyHostToDevice, st), "copy");
+  if (rc != HFG_OK) return rc;
+  for (size_t s = 0; s < ax.shells.shells.size(); ++s) ax.by_l[ax.shells.shells[s].l].push_back((int)s);
+  for (auto& kv : ax.by_l) {
+    rc = cuda_check(ctx, ax.idx[kv.first].alloc(kv.second.size()), "alloc");
+    if (rc == HFG_OK)
+      rc = cuda_check(ctx, cudaMemcpyAsync(ax.idx[kv.first].p, kv.second.data(), kv.second.size() * 4,
+                                           cudaMemcpyHostToDevice, st), "copy");
+    if (rc != HFG_OK) return rc;
+  }
+  // the host copies above are pageable: complete them before they go away
+  return cuda_check(ctx, cudaStreamSynchronize(st), "aux set");
+}
+
 int gemm_ex(hfg_ctx* ctx, cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
             const void* A, cudaDataType ta_t, int lda, const void* B, cudaDataType tb_t, int ldb, float beta,
             float* C, int ldc, cublasComputeType_t ct) {
@@ -87,45 +142,16 @@ int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, doubl
     if (rc != HFG_OK) return rc;         \
   } while (0)
   // auxiliary shells and their unit-partner "pairs"
-  hfg_ctx auxc;
-  rc = build_shell_list(&auxc, aux, 4);
-  if (rc != HFG_OK) return set_error(ctx, rc, "auxiliary basis: " + auxc.err);
+  AuxSet ax;
+  rc = make_aux_set(ctx, aux, ax);
+  if (rc != HFG_OK) return rc;
+  hfg_ctx& auxc = ax.shells;
   const int naux = auxc.n;
   df->naux = naux;
-  std::vector<PairInfo> upairs(auxc.shells.size());
-  std::vector<PrimPair> uprims;
-  for (size_t s = 0; s < auxc.shells.size(); ++s) {
-    const Shell& sh = auxc.shells[s];
-    PairInfo& pi = upairs[s];
-    pi = PairInfo{};
-    pi.Ax = sh.c[0];
-    pi.Ay = sh.c[1];
-    pi.Az = sh.c[2];
-    pi.ao_a = sh.ao;
-    pi.pp_off = (int)uprims.size();
-    pi.npp = sh.K;
-    for (int q = 0; q < sh.K; ++q) {
-      PrimPair p{};
-      p.p = auxc.exps[sh.prim_off + q];
-      p.inv_p = 1.0 / p.p;
-      p.kp = auxc.coefs[sh.prim_off + q] * p.inv_p;  // unit partner: coefficient 1, exp(0) = 1
-      uprims.push_back(p);
-    }
-  }
-  DevBuf<PairInfo> dup;
-  DevBuf<PrimPair> dupr;
-  CK(dup.alloc(upairs.size()));
-  CK(dupr.alloc(uprims.size()));
-  CK(cudaMemcpyAsync(dup.p, upairs.data(), upairs.size() * sizeof(PairInfo), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(dupr.p, uprims.data(), uprims.size() * sizeof(PrimPair), cudaMemcpyHostToDevice, st));
-  std::map<int, std::vector<int>> aux_by_l;
-  for (size_t s = 0; s < auxc.shells.size(); ++s) aux_by_l[auxc.shells[s].l].push_back((int)s);
-  std::map<int, DevBuf<int>> aux_idx;
-  for (auto& kv : aux_by_l) {
-    CK(aux_idx[kv.first].alloc(kv.second.size()));
-    CK(cudaMemcpyAsync(aux_idx[kv.first].p, kv.second.data(), kv.second.size() * 4, cudaMemcpyHostToDevice, st));
-  }
-
+  DevBuf<PairInfo>& dup = ax.dup;
+  DevBuf<PrimPair>& dupr = ax.dupr;
+  std::map<int, std::vector<int>>& aux_by_l = ax.by_l;
+  std::map<int, DevBuf<int>>& aux_idx = ax.idx;
   // metric (P|Q): bra and ket both unit-paired auxiliary shells
   CK(df->metric.alloc((size_t)naux * naux));
   for (auto& bk : aux_by_l) {
@@ -301,6 +327,78 @@ int hfg_df_metric(hfg_df* df, double* M) {
   const size_t len = (size_t)df->naux * df->naux;
   if (cudaMemcpy(M, df->metric.p, len * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
     return set_error(df->ctx, HFG_ERR_CUDA, "copy metric");
+  return HFG_OK;
+}
+
+// three_center_integrals (src/df.rs:60-78): (P|mu nu) for every auxiliary
+// function P (rows) and every AO pair mu >= nu (packed columns
+// compound_index(mu, nu) = mu (mu + 1) / 2 + nu), row-major, unscreened.
+int hfg_df_three_center(hfg_ctx* ctx, const hfg_basis* aux, double* out, size_t len) {
+  if (!ctx) return HFG_ERR_INVALID_INPUT;
+  if (!aux || !out) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  AllocScope alloc_scope(ctx->stream);
+  cudaStream_t st = ctx->stream;
+  AuxSet ax;
+  int rc = make_aux_set(ctx, aux, ax);
+  if (rc != HFG_OK) return rc;
+  const int naux = ax.shells.n;
+  const long long n = ctx->n, np = n * (n + 1) / 2;
+  if (len != (size_t)naux * (size_t)np)
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "three-centre length must be n_aux * n (n + 1) / 2");
+  // every shell pair's block in its own columns (as the factor build lays
+  // them out), then scattered to the packed AO-pair order on the host
+  std::vector<int2> colmn;
+  std::map<std::pair<int, int>, std::pair<std::vector<int>, std::vector<long long>>> by_class;
+  long long ncol = 0;
+  for (size_t i = 0; i < ctx->h_pairs.size(); ++i) {
+    const PairInfo& pi = ctx->h_pairs[i];
+    const PairClass& c = ctx->classes[pi.cls];
+    const int na = (c.la + 1) * (c.la + 2) / 2, nb = (c.lb + 1) * (c.lb + 2) / 2;
+    auto& e = by_class[{c.la, c.lb}];
+    e.first.push_back((int)i);
+    e.second.push_back(ncol);
+    for (int a = 0; a < na; ++a)
+      for (int b = 0; b < nb; ++b) {
+        if (pi.same && b > a) continue;
+        colmn.push_back(make_int2(pi.ao_a + a, pi.ao_b + b));
+      }
+    ncol += pi.same ? na * (na + 1) / 2 : na * nb;
+  }
+  if (ncol != np) return set_error(ctx, HFG_ERR_INTEGRAL, "AO pair count mismatch");
+  DevBuf<double> T3;
+  rc = cuda_check(ctx, T3.alloc((size_t)naux * ncol), "alloc three-centre");
+  if (rc != HFG_OK) return rc;
+  for (auto& bc : by_class) {
+    DevBuf<int> bidx;
+    DevBuf<long long> bcol;
+    rc = cuda_check(ctx, bidx.alloc(bc.second.first.size()), "alloc");
+    if (rc == HFG_OK) rc = cuda_check(ctx, bcol.alloc(bc.second.second.size()), "alloc");
+    if (rc == HFG_OK)
+      rc = cuda_check(ctx, cudaMemcpyAsync(bidx.p, bc.second.first.data(), bc.second.first.size() * 4,
+                                           cudaMemcpyHostToDevice, st), "copy");
+    if (rc == HFG_OK)
+      rc = cuda_check(ctx, cudaMemcpyAsync(bcol.p, bc.second.second.data(), bc.second.second.size() * 8,
+                                           cudaMemcpyHostToDevice, st), "copy");
+    for (auto& kk : ax.by_l) {
+      if (rc != HFG_OK) break;
+      Df3cArgs a{ctx->d_pairs.p, ctx->d_prims.p, bidx.p, bcol.p, (int)bc.second.first.size(), ax.dup.p, ax.dupr.p,
+                 ax.idx[kk.first].p, (int)kk.second.size(), ctx->d_boys64.p, ctx->d_expt64.p, T3.p, ncol};
+      rc = cuda_check(ctx, launch_df3c(bc.first.first, bc.first.second, kk.first, a, st), "three-centre kernel");
+    }
+    if (rc == HFG_OK) rc = cuda_check(ctx, cudaStreamSynchronize(st), "three-centre");
+    if (rc != HFG_OK) return rc;
+  }
+  std::vector<double> h((size_t)naux * ncol);
+  rc = cuda_check(ctx, cudaMemcpyAsync(h.data(), T3.p, h.size() * 8, cudaMemcpyDeviceToHost, st), "copy back");
+  if (rc == HFG_OK) rc = cuda_check(ctx, cudaStreamSynchronize(st), "three-centre");
+  if (rc != HFG_OK) return rc;
+  for (long long c = 0; c < ncol; ++c) {
+    const long long mu = std::max(colmn[c].x, colmn[c].y), nu = std::min(colmn[c].x, colmn[c].y);
+    const long long k = mu * (mu + 1) / 2 + nu;
+    for (int p = 0; p < naux; ++p) out[(size_t)p * np + k] = h[(size_t)p * ncol + c];
+  }
   return HFG_OK;
 }
 

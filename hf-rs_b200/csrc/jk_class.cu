@@ -1,6 +1,8 @@
 // One angular class of the J/K kernels, compiled once per class with
 // -DHFG_LA=.. -DHFG_LB=.. -DHFG_LC=.. -DHFG_LD=.. so the 21 classes build in
 // parallel.  Exports launch_jk_<LA><LB><LC><LD>().
+#include <atomic>
+
 #include "jk_dispatch.h"
 #include "jk_kernels.cuh"
 
@@ -19,14 +21,21 @@ static cudaError_t launch_t(const JKLaunchArgs& a, cudaStream_t st) {
   (void)L;
   const size_t smem = boys_smem_bytes<T>();
   auto kern = jk_kernel<HFG_LA, HFG_LB, HFG_LC, HFG_LD, T, NS, G>;
-  static int resident = [&] {
-    int dev = 0, sms = 0, per_sm = 0;
+  // resident blocks per device (a process may drive different device
+  // models), looked up once per device
+  constexpr int kMaxDev = 64;
+  static std::atomic<int> resident_by_dev[kMaxDev];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int resident = (dev >= 0 && dev < kMaxDev) ? resident_by_dev[dev].load(std::memory_order_relaxed) : 0;
+  if (resident <= 0) {
+    int sms = 0, per_sm = 0;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem);
-    return sms * (per_sm > 0 ? per_sm : 1);
-  }();
+    resident = sms * (per_sm > 0 ? per_sm : 1);
+    if (dev >= 0 && dev < kMaxDev) resident_by_dev[dev].store(resident, std::memory_order_relaxed);
+  }
   const long long want = (a.nchunks + (block / 32) - 1) / (block / 32);
   const long long grid = want < resident ? want : resident;
   if (grid <= 0) return cudaSuccess;

@@ -1,24 +1,28 @@
 // hfg_jk_device_noalloc: the direct J/K build without any device allocation.
 //
 // Who needs this: callers that must not allocate device memory while they
-// run -- code executing inside a CUDA stream capture (cudaMalloc is not
-// capturable and would end the capture), real-time or latency-bound
-// loops that cannot afford cudaMalloc's implicit device synchronisation,
-// and hosts whose device memory is entirely handed out by their own
-// allocator.  hfg_jk_device keeps its unsymmetrised J'/K' accumulators and
-// work-queue counters in buffers it allocates on first use; this entry
-// point keeps them instead in one file-scope device array, reserved when
-// the library is loaded and held by every GPU that loads it until the
-// process exits.
+// run -- latency-bound loops that cannot afford cudaMalloc's implicit device
+// synchronisation, and host programs whose device memory is entirely handed
+// out by their own allocator (a framework's caching pool that reserves the
+// GPU up front), where a cudaMalloc from this library would fail or steal
+// memory the host has promised elsewhere.  hfg_jk_device keeps its
+// unsymmetrised J'/K' accumulators and work-queue counters in buffers it
+// allocates on first use; this entry point keeps them instead in one
+// file-scope device array, reserved when the library is loaded and held by
+// every GPU that loads it until the process exits.
 //
-// Limit: the array holds 8 MiB, i.e. 512 bytes of work-queue counters plus
-// (1 + nspin) * n^2 doubles of accumulators, so n <= 724 for RHF and n <= 591
-// for UHF.  Larger systems are rejected with HFG_ERR_INVALID_INPUT.
+// Limit: the array holds 8 MiB: the plan's work-queue counters (8 bytes per
+// launch, rounded up to 256 bytes) plus (1 + nspin) * n^2 doubles of
+// accumulators, so n <= 724 for RHF and n <= 591 for UHF (for plans of up to
+// 224 launches; an s/p/d basis needs at most 42).  Larger systems are
+// rejected with HFG_ERR_INVALID_INPUT.
 //
-// Every call on a device shares the one array and it keeps the previous
-// call's contents, so each call clears the counters and accumulators first;
-// calls that overlap on the GPU (several host threads, or several streams)
-// race on the array and must be serialised by the caller.
+// The first call on a device looks up the array's device address (once per
+// device, with that device current); make that first call before any stream
+// capture.  Every call on a device shares the one array and it keeps the
+// previous call's contents, so each call clears the counters and
+// accumulators first; calls that overlap on the GPU (several host threads, or
+// several streams) race on the array and must be serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -29,7 +33,6 @@
 namespace {
 
 constexpr size_t kScratchBytes = 8u << 20;
-constexpr size_t kCounterBytes = 512;  // room for 64 work-queue counters
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_jk_scratch[kScratchBytes];
@@ -69,15 +72,21 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
   if (!ctx) return HFG_ERR_INVALID_INPUT;
   if (!dPt || !dPs || !dJ || !dK) return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
   if (nspin < 1 || nspin > 2) return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, "nspin must be 1 or 2");
-  std::lock_guard<std::mutex> lk(ctx->mu);
-  const size_t nn = (size_t)ctx->n * ctx->n;
-  const size_t need = kCounterBytes + (size_t)(1 + nspin) * nn * sizeof(double);
-  if (need > kScratchBytes)
-    return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT,
-                          "hfg_jk_device_noalloc: (1 + nspin) * n^2 doubles exceed its 8 MiB scratch "
-                          "(n <= 724 for RHF, n <= 591 for UHF); use hfg_jk_device");
   hfg_jk_opts o;
   if (opts) o = *opts; else hfg_jk_opts_default(&o);
+  // the same checks as hfg_jk_device, before the plan lookup (a NaN key
+  // would break the ordering of the plan map)
+  if (!(o.schwarz_threshold >= 0.0) || !(o.prim_threshold >= 0.0) ||
+      (o.precision != HFG_FP64 && o.precision != HFG_MIXED) ||
+      (o.precision == HFG_MIXED && !(o.mixed_threshold >= 0.0)))
+    return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid J/K options");
+  const size_t nn = (size_t)ctx->n * ctx->n;
+  const char* too_big =
+      "hfg_jk_device_noalloc: (1 + nspin) * n^2 doubles and the work-queue counters exceed its 8 MiB scratch "
+      "(n <= 724 for RHF, n <= 591 for UHF); use hfg_jk_device";
+  if (256 + (size_t)(1 + nspin) * nn * sizeof(double) > kScratchBytes)
+    return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, too_big);
+  std::lock_guard<std::mutex> lk(ctx->mu);
   auto it = ctx->plans.find(std::make_tuple(o.schwarz_threshold, o.precision == HFG_MIXED ? o.mixed_threshold : 0.0,
                                             o.prim_threshold, o.precision));
   if (it == ctx->plans.end())
@@ -85,15 +94,18 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
                           "hfg_jk_device_noalloc: no launch plan for these options on this context; call hfg_jk or "
                           "hfg_jk_device once with them first (that call allocates the plan)");
   const hfg::Plan& plan = *it->second;
-  if (plan.launches.size() * sizeof(unsigned long long) > kCounterBytes)
-    return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, "hfg_jk_device_noalloc: too many launches for the scratch");
+  // counters first (one per launch, rounded up to keep the accumulators
+  // 256-byte aligned), then J' and K'
+  const size_t counter_bytes = (plan.launches.size() * sizeof(unsigned long long) + 255) / 256 * 256;
+  const size_t need = counter_bytes + (size_t)(1 + nspin) * nn * sizeof(double);
+  if (need > kScratchBytes) return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, too_big);
   if (cudaSetDevice(ctx->device) != cudaSuccess) return hfg::set_error(ctx, HFG_ERR_CUDA, "cudaSetDevice");
   void* base = nullptr;
   int rc = scratch_address(ctx, ctx->device, &base);
   if (rc != HFG_OK) return rc;
   unsigned char* b = static_cast<unsigned char*>(base);
   unsigned long long* counters = reinterpret_cast<unsigned long long*>(b);
-  double* Jacc = reinterpret_cast<double*>(b + kCounterBytes);
+  double* Jacc = reinterpret_cast<double*>(b + counter_bytes);
   double* Kacc = Jacc + nn;
   // the array keeps the last call's contents: clear counters and accumulators
   rc = hfg::cuda_check(ctx, cudaMemsetAsync(b, 0, need, ctx->stream), "scratch clear");

@@ -163,6 +163,7 @@ def load_library():
     L.hfg_df_destroy.argtypes = [VP]
     L.hfg_df_sizes.argtypes = [VP, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_longlong)]
     L.hfg_df_metric.argtypes = [VP, DP]
+    L.hfg_df_three_center.argtypes = [VP, P(HfgBasis), DP, ctypes.c_size_t]
     L.hfg_df_jk.argtypes = [VP, DP, ctypes.c_int, DP, DP, ctypes.c_int]
     L.hfg_scf_df.argtypes = [VP, VP, ctypes.c_int, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     L.hfg_server_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, P(VP)]
@@ -370,6 +371,16 @@ class Context:
             self._check(rc)
         out = r.as_dict()
         out.update({"P": P, "F": F, "J": J, "K": K, "status": rc})
+        return out
+
+    def df_three_center(self, aux):
+        """(P|mu nu) for every auxiliary function and AO pair mu >= nu
+        (hfg_df_three_center): naux x n (n + 1) / 2, packed columns."""
+        b = HfgBasis(aux.n, _dp(aux.center), _ip(aux.lxyz), _ip(aux.atom), _ip(aux.prim_off), _dp(aux.exps),
+                     _dp(aux.coefs))
+        np_ = self.n * (self.n + 1) // 2
+        out = np.zeros((aux.n, np_))
+        self._check(self.lib.hfg_df_three_center(self.h, ctypes.byref(b), _dp(out), out.size))
         return out
 
     def last_stats(self):

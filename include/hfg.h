@@ -133,18 +133,20 @@ int hfg_jk_device(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double
 
 /*
  * No counterpart in hf-rs.  As hfg_jk_device, but allocates no device
- * memory at all, for callers that cannot allocate while they run (inside
- * a CUDA stream capture, in latency-bound loops that cannot take
- * cudaMalloc's device synchronisation, or under an allocator that owns all
- * device memory).  The J'/K' accumulators and work-queue counters live in
- * one 8 MiB device array that the library reserves when it is loaded, so
- * (1 + nspin) * n^2 doubles must fit: n <= 724 (RHF), n <= 591 (UHF); larger
- * systems return HFG_ERR_INVALID_INPUT.  The launch plan for `opts` must
- * already exist on the context (one earlier hfg_jk or hfg_jk_device call
- * with the same options builds it).  The first call on a device looks up
- * the array's device address; make that first call before any stream
- * capture.  All calls on a device share the array: calls that overlap on
- * the GPU race and must be serialised by the caller.
+ * memory at all, for callers that cannot allocate while they run:
+ * latency-bound loops that cannot take cudaMalloc's device synchronisation,
+ * and host programs whose own allocator has reserved all device memory.
+ * The J'/K' accumulators and work-queue counters live in one 8 MiB device
+ * array that the library reserves when it is loaded, so (1 + nspin) * n^2
+ * doubles plus 8 bytes per launch of the plan (rounded up to 256) must fit:
+ * n <= 724 (RHF), n <= 591 (UHF); larger systems return
+ * HFG_ERR_INVALID_INPUT.  The launch plan for `opts` must already exist on
+ * the context (one earlier hfg_jk or hfg_jk_device call with the same
+ * options builds it).  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  All calls
+ * on a device share the array, which keeps the last call's contents (each
+ * call clears what it uses first): calls that overlap on the GPU race and
+ * must be serialised by the caller.
  */
 int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* d_P_total,
                           const double* d_P_spin, double* d_J, double* d_K);
@@ -222,6 +224,14 @@ int hfg_df_destroy(hfg_df* df);
 int hfg_df_sizes(const hfg_df* df, int* naux, int* rank, long long* ncol);
 /* The metric (P|Q) as built (naux x naux, row-major). */
 int hfg_df_metric(hfg_df* df, double* M);
+/*
+ * Stands in for three_center_integrals (src/df.rs:60-78): (P|mu nu) of every
+ * auxiliary function P of `aux` (rows) and every AO pair mu >= nu of the
+ * context's basis (packed columns compound_index(mu, nu), src/scf.rs:222),
+ * row-major, len = n_aux * n (n + 1) / 2, unscreened.  Meant for inspection
+ * and small systems (the factor build never forms this matrix whole).
+ */
+int hfg_df_three_center(hfg_ctx* ctx, const hfg_basis* aux, double* out, size_t len);
 /*
  * Stands in for DfTensor::coulomb_exchange_rhf (src/df.rs:133-174): J and K
  * of the density 2 C_occ C_occ^T, C_occ row-major n x nocc (host).  `mma`

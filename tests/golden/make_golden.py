@@ -1,9 +1,10 @@
 """Copy the hf-rs golden vectors for the Fock-build path into small fixtures.
 
 hf-rs keeps PySCF/mpmath-generated reference values under tests/data/ of its
-own tree.  This script reads them (from a local hf-rs checkout, default
-/root/reference) and writes the subsets the parity tests here need, so that
-the tests run without the reference tree:
+own tree.  This script reads them from a local hf-rs checkout, whose root is
+its one required argument (python make_golden.py <hf-rs root>), and writes the
+subsets the parity tests here need, so that the tests run without the
+reference tree:
 
   boys.json          tests/data/boys_reference.json (all 31 T values, n<=40)
   spdf_eri.npz       spherical_reference.json["spdf_integrals"]: the basis
@@ -11,8 +12,9 @@ the tests run without the reference tree:
                      Cartesian ERIs with their (i,j,k,l) indices
   scf_energies.json  scf_reference.json: RHF/UHF energies (STO-3G, 6-31G*)
   water_ccpvdz.json  spherical_reference.json["systems"]["water_ccpvdz"]
-  df.npz             df_reference.json: metric and (P|mn) for water STO-3G /
-                     def2-SVP-RI, and the df_hf_reference.json "water" case
+  df.npz             df_reference.json: metric, (P|mn) and the RI-MP2 energy
+                     for water STO-3G / def2-SVP-RI, and the
+                     df_hf_reference.json "water" case
 """
 import json
 import os
@@ -65,9 +67,11 @@ def main(root):
     np.savez_compressed(os.path.join(HERE, "df.npz"), metric=np.array(df["metric"]),
                         three=np.array(df["three"]), water_atoms=np.array(json.dumps(c["atoms"])),
                         e_scf=c["e_scf"], P=np.array(c["density"]), F=np.array(c["fock"]),
-                        J=np.array(c["j"]), K=np.array(c["k"]), n_aux=c["n_aux"])
+                        J=np.array(c["j"]), K=np.array(c["k"]), n_aux=c["n_aux"], ri_mp2=df["ri_mp2"])
     print("fixtures written to", HERE)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <hf-rs checkout root>")
+    main(sys.argv[1])

@@ -28,3 +28,21 @@ def test_admission_by_footprint_limits_concurrency():
     starts = sorted((r["start_ms"], r["end_ms"]) for r in res)
     assert any(s2 >= e1 for (s1, e1), (s2, e2) in zip(starts, starts[1:]))
     assert all(r["status"] == 0 for r in res)
+
+
+def test_mixed_jobs_same_alone_and_in_the_mix_with_arrivals():
+    # the served precision policy (mixed J/K with FP64 refinement, here for
+    # every job) and arrivals honoured: jobs enter while others are running,
+    # and each converged energy equals the job's energy run alone
+    from hfgpu.serve import MIXED
+    jobs = make_stream(10, rate=25.0, max_waters=6, seed=11)
+    inputs = build_inputs(jobs)
+    alone, _ = run_stream(jobs, slots=1, budget_bytes=8 << 30, honour_arrivals=False, inputs=inputs, jk=MIXED,
+                          mixed_min_ao=0)
+    mixed, span = run_stream(jobs, slots=4, budget_bytes=8 << 30, honour_arrivals=True, inputs=inputs, jk=MIXED,
+                             mixed_min_ao=0)
+    assert all(r["status"] == 0 and r["converged"] for r in alone + mixed)
+    for a, m in zip(alone, mixed):
+        assert abs(a["energy"] - m["energy"]) < 1e-9, (a["tag"], a["energy"], m["energy"])
+    # some job was submitted while another was already running
+    assert any(o["start_ms"] < m["submit_ms"] < o["end_ms"] for m in mixed for o in mixed if o is not m)

@@ -1,10 +1,9 @@
 """The allocation-free J/K entry point (hfg_jk_device_noalloc).
 
-Some callers cannot allocate device memory while they run -- code inside a
-CUDA stream capture, latency-bound loops that cannot take cudaMalloc's device
-synchronisation, hosts whose allocator owns all device memory.  This entry
-point serves them from an 8 MiB device array the library reserves at load
-time.  These tests call it through the C ABI and check it against the
+Some callers cannot allocate device memory while they run -- latency-bound
+loops that cannot take cudaMalloc's device synchronisation, and host programs
+whose own allocator has reserved all device memory.  This entry point serves
+them from an 8 MiB device array the library reserves at load time.  These tests call it through the C ABI and check it against the
 ordinary entry point, on two calls in a row (the array is shared and keeps
 the previous call's contents, so the second call checks that it is cleared).
 This file is named to be collected last.
@@ -34,14 +33,16 @@ def noalloc(ctx, opts, nspin, Pt, Ps, J, K):
     return rc
 
 
+@pytest.mark.parametrize("mixed", [None, 1e-6])
 @pytest.mark.parametrize("nspin", [1, 2])
-def test_noalloc_matches_jk_on_two_calls(nspin):
+def test_noalloc_matches_jk_on_two_calls(nspin, mixed):
     import torch
     atoms = water_cluster(2)
     basis = CartesianBasis.build(atoms, "cc-pvdz")
     n = basis.n
     ctx = Context(basis)
-    opts = JKOptions.make()
+    # FP64, and mixed precision (twice as many launches, so twice the counters)
+    opts = JKOptions.make(mixed=mixed)
     dev = torch.device("cuda", 0)
     for call, seed in enumerate((11, 12)):
         Pa, Pb = rand_sym(n, seed), rand_sym(n, seed + 100)
