@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-jobs", type=int, default=24)
     ap.add_argument("--serve-max-waters", type=int, default=16)
-    ap.add_argument("--df-waters", type=int, default=32, help="also time DF J/K on (H2O)_n (0: skip)")
+    ap.add_argument("--df-waters", type=int, default=48, help="also time DF J/K on (H2O)_n (0: skip)")
     ap.add_argument("--scf-waters", type=int, default=-1,
                     help="full SCF in FP64 and in the mixed form on (H2O)_n (-1: --waters, 0: skip)")
     ap.add_argument("--jk-only", action="store_true",
@@ -544,38 +544,73 @@ def measure_scf(waters, ctx, opt_mixed):
 
 
 def measure_df(args, torch):
-    """DF J/K (hfg_df_jk) on (H2O)_n cc-pVDZ with def2-universal-JKFIT: build
-    time and J/K time per precision, and K-GEMM throughput (4 n^2 naux nocc
-    flops per build)."""
-    import time as _t
+    """DF J/K (hfg_df_jk) on (H2O)_n cc-pVDZ with def2-universal-JKFIT.
+
+    The FP64-stored factor with FP64 arithmetic is the reference; the
+    FP32-stored factor runs the exchange on the tensor cores (this library's
+    tcgen05 kernels) with TF32 and with BF16 operands.  Per form: factor
+    build time, J/K wall time, the exchange's device time and executed
+    tensor-core TFLOP/s (both GEMMs, zero tiles skipped, lower triangle of K),
+    the reference's algorithmic rate (4 n^2 nocc naux flops), the fraction
+    of the measured BF16 tensor peak (TF32 runs at half of it), the error of
+    K against the FP64 form, and the same J/K through cuBLAS GEMMs on the
+    same factor (HFG_DF_K_CUBLAS=1) for comparison."""
     import numpy as np
     from hfgpu import CartesianBasis, Context
     from hfgpu.clusters import water_cluster
     from hfgpu.lib import HFG_DF_BF16, HFG_DF_FP32, HFG_DF_FP64, DFTensor
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    bf16_peak = peaks.get("bf16_tflops_sustained") or 1356.3
     atoms = water_cluster(args.df_waters)
     ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
     aux = CartesianBasis.build(atoms, "def2-universal-jkfit")
     n, nocc = ctx.n, 5 * args.df_waters
     q, _ = np.linalg.qr(np.random.default_rng(5).standard_normal((n, nocc)))
-    out = {"waters": args.df_waters, "n_ao": n, "naux": aux.n, "nocc": nocc}
-    ref = None
-    for name, storage in [("fp64", HFG_DF_FP64), ("tf32", HFG_DF_FP32), ("bf16", HFG_DF_BF16)]:
-        t0 = _t.time()
-        df = DFTensor(ctx, aux, pair_threshold=1e-12, storage=storage)
-        tb = _t.time() - t0
-        df.jk(q, mma=storage)
-        t0 = _t.time()
-        J, K = df.jk(q, mma=storage)
-        tj = _t.time() - t0
-        if ref is None:
-            ref = (J, K)
-        naux, rank, ncol = df.sizes()
-        out[name] = {"build_s": tb, "jk_s": tj, "rank": rank, "pairs": ncol,
-                     "k_gemm_tflops": 4.0 * n * n * rank * nocc / tj / 1e12,
-                     "max_abs_dJ_vs_fp64": float(np.max(np.abs(J - ref[0]))),
-                     "max_abs_dK_vs_fp64": float(np.max(np.abs(K - ref[1])))}
-        df.close()
-    out["k_tflops_best"] = max(out[k]["k_gemm_tflops"] for k in ("tf32", "bf16"))
+    out = {"waters": args.df_waters, "n_ao": n, "naux": aux.n, "nocc": nocc,
+           "peak_tflops_bf16_sustained": bf16_peak, "peak_source": "MEASURED_PEAKS.json" if peaks else "fallback"}
+
+    def wall(fn, reps=3):
+        fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.time()
+            r = fn()
+            ts.append(time.time() - t0)
+        return min(ts), r
+
+    t0 = time.time()
+    d64 = DFTensor(ctx, aux, pair_threshold=1e-12, storage=HFG_DF_FP64)
+    out["fp64"] = {"build_s": time.time() - t0}
+    t64, (J64, K64) = wall(lambda: d64.jk(q, mma=HFG_DF_FP64), reps=2)
+    naux, rank, ncol = d64.sizes()
+    out["fp64"].update({"jk_s": t64, "rank": rank, "pairs": ncol, "arith": "FP64 (cuBLAS DGEMM)"})
+    d64.close()
+    t0 = time.time()
+    d32 = DFTensor(ctx, aux, pair_threshold=1e-12, storage=HFG_DF_FP32)
+    build32 = time.time() - t0
+    alg = 4.0 * n * n * nocc * rank
+    best = 0.0
+    for name, mma, scale in (("tf32", HFG_DF_FP32, 0.5), ("bf16", HFG_DF_BF16, 1.0)):
+        tj, (J, K) = wall(lambda: d32.jk(q, mma=mma))
+        st = d32.last_stats()
+        ex = st["k_flops"] / (st["k_ms"] * 1e-3) / 1e12
+        os.environ["HFG_DF_K_CUBLAS"] = "1"
+        tc, (Jc, Kc) = wall(lambda: d32.jk(q, mma=mma))
+        del os.environ["HFG_DF_K_CUBLAS"]
+        out[name] = {"factor": "FP32", "build_s": build32, "jk_s": tj, "k_ms": st["k_ms"],
+                     "k_tflops_executed": ex, "k_tflops_algorithmic": alg / (st["k_ms"] * 1e-3) / 1e12,
+                     "tensor_peak_frac": ex / (bf16_peak * scale), "nonzero_tile_share": st["tiles_fraction"],
+                     "rel_err_K_vs_fp64": float(np.linalg.norm(K - K64) / np.linalg.norm(K64)),
+                     "max_abs_dJ_vs_fp64": float(np.max(np.abs(J - J64))),
+                     "cublas_jk_s": tc, "speedup_vs_cublas": tc / tj,
+                     "cublas_rel_err_K_vs_fp64": float(np.linalg.norm(Kc - K64) / np.linalg.norm(K64))}
+        best = max(best, ex)
+    d32.close()
+    out["k_tflops_best"] = best
+    ctx.close()
     return out
 
 

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "df_internal.h"
+#include "df_umma.h"
 #include "hfg_ctx.h"
 
 using namespace hfg;
@@ -44,7 +45,19 @@ struct hfg_df {
   DevBuf<float> gam32, jcol32, pvec32, Kf, Tf, Cf;
   DevBuf<__nv_bfloat16> Cb, Tb;
   DevBuf<unsigned char> dense;
+  // tensor-core exchange: tile structure of the unpacked factor per operand
+  // type (built on first use) and its scratch
+  TileStructure tiles[2];
+  bool tiles_ready[2] = {false, false};
+  DevBuf<int> tile_off[2], tile_kt[2], tile_map[2];
+  UmmaWorkspace uws;
+  // device time of the last exchange (K) and its executed tensor-core flops
+  cudaEvent_t kev[2] = {nullptr, nullptr};
+  double k_flops = 0.0, tiles_fraction = 0.0;
+  bool k_timed = false;
   ~hfg_df() {
+    for (auto& e : kev)
+      if (e) cudaEventDestroy(e);
     if (blas) cublasDestroy(blas);
   }
 };
@@ -114,6 +127,33 @@ int gemm_ex(hfg_ctx* ctx, cublasHandle_t h, cublasOperation_t ta, cublasOperatio
       cublasGemmEx(h, ta, tb, m, n, k, &alpha, A, ta_t, lda, B, tb_t, ldb, &beta, C, CUDA_R_32F, ldc, ct,
                    CUBLAS_GEMM_DEFAULT);
   return s == CUBLAS_STATUS_SUCCESS ? HFG_OK : set_error(ctx, HFG_ERR_CUDA, "cublasGemmEx failed");
+}
+
+int ensure_tiles(hfg_df* df, int kind) {
+  if (df->tiles_ready[kind]) return HFG_OK;
+  hfg_ctx* ctx = df->ctx;
+  std::vector<int2> colmn((size_t)df->ncol);
+  int rc = cuda_check(ctx, cudaMemcpy(colmn.data(), df->colmn.p, colmn.size() * sizeof(int2), cudaMemcpyDeviceToHost),
+                      "copy pair map");
+  if (rc != HFG_OK) return rc;
+  TileStructure& t = df->tiles[kind];
+  t.build(colmn, df->n, kind);
+  auto up = [&](DevBuf<int>& d, const std::vector<int>& h) -> int {
+    int r = cuda_check(ctx, d.alloc(std::max<size_t>(1, h.size())), "alloc tile structure");
+    if (r == HFG_OK && !h.empty())
+      r = cuda_check(ctx, cudaMemcpyAsync(d.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
+                     "copy tile structure");
+    return r;
+  };
+  if ((rc = up(df->tile_off[kind], t.tile_off)) != HFG_OK) return rc;
+  if ((rc = up(df->tile_kt[kind], t.tile_kt)) != HFG_OK) return rc;
+  if ((rc = up(df->tile_map[kind], t.tile_map)) != HFG_OK) return rc;
+  rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "tile structure");
+  if (rc != HFG_OK) return rc;
+  t.tile_map.clear();
+  t.tile_map.shrink_to_fit();
+  df->tiles_ready[kind] = true;
+  return HFG_OK;
 }
 
 }  // namespace
@@ -330,6 +370,20 @@ int hfg_df_metric(hfg_df* df, double* M) {
   return HFG_OK;
 }
 
+int hfg_df_last_stats(hfg_df* df, double* k_ms, double* k_flops, double* tiles_fraction) {
+  if (!df) return HFG_ERR_INVALID_INPUT;
+  if (!df->k_timed) return set_error(df->ctx, HFG_ERR_INVALID_INPUT, "no tensor-core exchange has run on this factor");
+  cudaSetDevice(df->ctx->device);
+  float ms = 0.f;
+  int rc = cuda_check(df->ctx, cudaEventSynchronize(df->kev[1]), "exchange event");
+  if (rc == HFG_OK) rc = cuda_check(df->ctx, cudaEventElapsedTime(&ms, df->kev[0], df->kev[1]), "exchange time");
+  if (rc != HFG_OK) return rc;
+  if (k_ms) *k_ms = ms;
+  if (k_flops) *k_flops = df->k_flops;
+  if (tiles_fraction) *tiles_fraction = df->tiles_fraction;
+  return HFG_OK;
+}
+
 // three_center_integrals (src/df.rs:60-78): (P|mu nu) for every auxiliary
 // function P (rows) and every AO pair mu >= nu (packed columns
 // compound_index(mu, nu) = mu (mu + 1) / 2 + nu), row-major, unscreened.
@@ -449,7 +503,53 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
   CK(cudaMemsetAsync(dJ, 0, nn * 8, st));
   CK(launch_unpack_j(df->jcol.p, df->colmn.p, ncol, n, dJ, st));
 
+  // K on the tensor cores: this library's tcgen05 kernels (df_umma.cu).
+  // HFG_DF_K_CUBLAS=1 selects the cuBLAS GEMMs below instead, kept only to
+  // time the two side by side.
+  const char* kc = getenv("HFG_DF_K_CUBLAS");
+  const bool k_cublas = kc && kc[0] == '1';
+  if (mma != HFG_DF_FP64 && !k_cublas) {
+    const int kind = mma == HFG_DF_BF16 ? kBF16 : kTF32;
+    rc = ensure_tiles(df, kind);
+    if (rc != HFG_OK) return rc;
+    UmmaDfArgs ua;
+    ua.device = ctx->device;
+    ua.n = n;
+    ua.nocc = nocc;
+    ua.rank = rank;
+    ua.kind = kind;
+    ua.storage = df->storage == HFG_DF_BF16 ? 2 : 1;
+    ua.ncol = ncol;
+    ua.B = df->storage == HFG_DF_BF16 ? (const void*)df->B16.p : (const void*)df->B32.p;
+    ua.C = dC;
+    ua.K = dK;
+    ua.tiles = &df->tiles[kind];
+    ua.tile_off_dev = df->tile_off[kind].p;
+    ua.tile_kt_dev = df->tile_kt[kind].p;
+    ua.tile_map_dev = df->tile_map[kind].p;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    ua.chunk_bytes = std::max<size_t>((size_t)64 << 20, std::min<size_t>((size_t)4 << 30, free_b / 4));
+    if (const char* ev = getenv("HFG_DF_K_CHUNK")) ua.max_chunk = atoi(ev);  // tests: many chunks
+    int status = 0;
+    if (!df->kev[0]) {
+      CK(cudaEventCreate(&df->kev[0]));
+      CK(cudaEventCreate(&df->kev[1]));
+    }
+    CK(cudaEventRecord(df->kev[0], st));
+    CK(df_k_tensor_cores(ua, df->uws, &status, st));
+    CK(cudaEventRecord(df->kev[1], st));
+    df->k_flops = df->uws.flops_executed;
+    df->tiles_fraction = df->uws.tiles_fraction;
+    df->k_timed = true;
+    if (status != 0)
+      return set_error(ctx, HFG_ERR_TIMEOUT, "DF exchange kernel: a bounded wait ran out (code " +
+                                                 std::to_string(status) + ")");
+    return HFG_OK;
+  }
+
   // K: chunks of qc auxiliary functions
+  df->k_timed = false;
   const size_t esz = mma == HFG_DF_FP64 ? 8 : (mma == HFG_DF_FP32 ? 4 : 2);
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);

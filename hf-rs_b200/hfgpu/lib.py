@@ -165,6 +165,7 @@ def load_library():
     L.hfg_df_metric.argtypes = [VP, DP]
     L.hfg_df_three_center.argtypes = [VP, P(HfgBasis), DP, ctypes.c_size_t]
     L.hfg_df_jk.argtypes = [VP, DP, ctypes.c_int, DP, DP, ctypes.c_int]
+    L.hfg_df_last_stats.argtypes = [VP, DP, DP, DP]
     L.hfg_scf_df.argtypes = [VP, VP, ctypes.c_int, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     L.hfg_server_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, P(VP)]
     L.hfg_server_submit.argtypes = [VP, P(Job)]
@@ -219,9 +220,19 @@ class Context:
             raise HfgError(rc, self.lib.hfg_last_error(self.h).decode())
 
     def close(self):
+        """Destroy the context; DF tensors built on it are destroyed first
+        (each holds a pointer into the context)."""
+        for child in list(getattr(self, "_children", ())):
+            child.close()
         if getattr(self, "h", None) is not None and self.h.value:
             self.lib.hfg_ctx_destroy(self.h)
             self.h = VP()
+
+    def _adopt(self, child):
+        import weakref
+        if not hasattr(self, "_children"):
+            self._children = weakref.WeakSet()
+        self._children.add(child)
 
     def __del__(self):
         try:
@@ -437,6 +448,7 @@ class DFTensor:
                                    ctypes.byref(h))
         ctx._check(rc)
         self.h = h
+        ctx._adopt(self)
 
     def sizes(self):
         a, r, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
@@ -456,10 +468,18 @@ class DFTensor:
         self.ctx._check(self.lib.hfg_df_jk(self.h, _dp(C), C.shape[1], _dp(J), _dp(K), mma))
         return J, K
 
+    def last_stats(self):
+        """Device time (ms), executed tensor-core flops and non-zero tile share
+        of the last tensor-core exchange (hfg_df_last_stats)."""
+        ms, fl, tf = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self.ctx._check(self.lib.hfg_df_last_stats(self.h, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(tf)))
+        return {"k_ms": ms.value, "k_flops": fl.value, "tiles_fraction": tf.value}
+
     def close(self):
-        if getattr(self, "h", None) is not None and self.h.value:
+        # a context that is already gone took its DF tensors with it
+        if getattr(self, "h", None) is not None and self.h.value and self.ctx.h.value:
             self.lib.hfg_df_destroy(self.h)
-            self.h = VP()
+        self.h = VP()
 
     def __del__(self):
         try:

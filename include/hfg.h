@@ -239,6 +239,13 @@ int hfg_df_three_center(hfg_ctx* ctx, const hfg_basis* aux, double* out, size_t 
  * FP32 accumulation, summed into FP64.
  */
 int hfg_df_jk(hfg_df* df, const double* C_occ, int nocc, double* J, double* K, int mma);
+/*
+ * No counterpart in hf-rs.  Device time (ms) of the exchange (K) of the last
+ * tensor-core hfg_df_jk on this factor, the tensor-core flops it executed
+ * (both GEMMs, zero tiles skipped, lower triangle of K only), and the share
+ * of the 128-row tiles of the unpacked B_Q that hold any stored AO pair.
+ */
+int hfg_df_last_stats(hfg_df* df, double* k_ms, double* k_flops, double* tiles_fraction);
 
 /* Options of hfg_scf: nuclei, electrons, AO space and convergence controls of
    run_scf_in_space_with_convergence / run_uhf_in_space_with_convergence
