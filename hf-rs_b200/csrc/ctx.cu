@@ -369,9 +369,9 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     return HFG_OK;
   }
   auto plan = std::make_unique<Plan>();
-  std::map<std::tuple<int, int, int, int, int, int>, int> lidx;
-  auto get_launch = [&](int la, int lb, int lc, int ld, int G, bool fp32) -> Launch& {
-    auto k = std::make_tuple(la, lb, lc, ld, G, (int)fp32);
+  std::map<std::tuple<int, int, int, int, int>, int> lidx;
+  auto get_launch = [&](int la, int lb, int lc, int ld, bool fp32) -> Launch& {
+    auto k = std::make_tuple(la, lb, lc, ld, (int)fp32);
     auto f = lidx.find(k);
     if (f != lidx.end()) return plan->launches[f->second];
     lidx[k] = (int)plan->launches.size();
@@ -380,7 +380,6 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     L.lb = lb;
     L.lc = lc;
     L.ld = ld;
-    L.G = G;
     L.fp32 = fp32;
     L.prefix.push_back(0);
     plan->launches.push_back(std::move(L));
@@ -396,9 +395,6 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     const PairClass& B = ctx->classes[cb];
     for (int ck = 0; ck <= cb; ++ck) {
       const PairClass& Kc = ctx->classes[ck];
-      const long kk = (long)B.Ka * B.Kb * Kc.Ka * Kc.Kb;
-      const int G = choose_group(B.la, B.lb, Kc.la, Kc.lb, kk);
-      const int qpw = 32 / G;
       const double w = wmd_flops(B.la, B.lb, Kc.la, Kc.lb);
       for (int i = B.first; i < B.first + B.count; ++i) {
         const double qi = Q[i];
@@ -421,9 +417,9 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
         for (int r = 0; r < 2; ++r) {
           const int a0 = ranges[r][0], a1 = ranges[r][1];
           if (a1 <= a0) continue;
-          Launch& L = get_launch(B.la, B.lb, Kc.la, Kc.lb, G, r == 1);
+          Launch& L = get_launch(B.la, B.lb, Kc.la, Kc.lb, r == 1);
           L.entries.push_back({i, Kc.first + a0, Kc.first + a1, 0});
-          L.prefix.push_back(L.prefix.back() + (a1 - a0 + qpw - 1) / qpw);
+          L.prefix.push_back(L.prefix.back() + (a1 - a0 + 31) / 32);
           const double nq = a1 - a0;
           const double npr = ctx->h_pairs[i].npp * (cum[Kc.first + a1] - cum[Kc.first + a0]);
           L.quartets += nq;
@@ -468,11 +464,10 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
       std::vector<JKEntry> ents(ne);
       std::vector<double> c2(ne);
       L.prefix.assign(1, 0);
-      const int qpw = 32 / L.G;
       for (size_t i = 0; i < ne; ++i) {
         ents[i] = L.entries[ord[i]];
         c2[i] = cost[ord[i]];
-        L.prefix.push_back(L.prefix.back() + (ents[i].k_hi - ents[i].k_lo + qpw - 1) / qpw);
+        L.prefix.push_back(L.prefix.back() + (ents[i].k_hi - ents[i].k_lo + 31) / 32);
       }
       L.entries.swap(ents);
       cost.swap(c2);
@@ -550,7 +545,7 @@ static int count_plan(hfg_ctx* ctx, Plan* plan) {
     HFG_CUDA(ctx, cudaMemsetAsync(cnt.p, 0, 2 * nl * 8, ctx->stream));
     for (size_t l = 0; l < nl; ++l) {
       const Launch& L = plan->launches[l];
-      HFG_CUDA(ctx, launch_count(L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1], L.G, ctx->d_pairs.p,
+      HFG_CUDA(ctx, launch_count(L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1], ctx->d_pairs.p,
                                  ctx->d_pairQ.p, thr, ctx->d_pbound.p, prim_eps, cnt.p + 2 * l, ctx->stream));
     }
     std::vector<unsigned long long> h(2 * nl);
@@ -709,7 +704,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
     a.nchunks = c1 - c0;
     a.nentries = (int)L.prefix[0];
     a.nwarps = L.prefix[1];
-    HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.G, L.fp32, a, ctx->stream));
+    HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.fp32, a, ctx->stream));
     if (profile) cudaEventRecord(ev[l + 1], ctx->stream);
   }
   if (profile) {
@@ -720,8 +715,8 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
       cudaEventElapsedTime(&ms, ev[l], ev[l + 1]);
       tot += ms;
       const Launch& L = plan->launches[l];
-      fprintf(stderr, "hfg-profile (%d%d|%d%d) G%-2d %s entries %8lld warps %10lld quartets %.3e prims %.3e  %9.3f ms  %.3e prim/s\n",
-              L.la, L.lb, L.lc, L.ld, L.G, L.fp32 ? "fp32" : "fp64", L.prefix[0], L.prefix[1], L.quartets, L.prims, ms,
+      fprintf(stderr, "hfg-profile (%d%d|%d%d) %s entries %8lld warps %10lld quartets %.3e prims %.3e  %9.3f ms  %.3e prim/s\n",
+              L.la, L.lb, L.lc, L.ld, L.fp32 ? "fp32" : "fp64", L.prefix[0], L.prefix[1], L.quartets, L.prims, ms,
               L.prims / (ms * 1e-3));
     }
     fprintf(stderr, "hfg-profile total %.3f ms\n", tot);
@@ -1003,7 +998,6 @@ static int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len
   if (rc != HFG_OK) return rc;
   HFG_CUDA(ctx, cudaMemsetAsync(d_out, 0, len * sizeof(double), ctx->stream));
   for (const Launch& L : plan->launches) {
-    if (L.G != 1) return set_error(ctx, HFG_ERR_UNSUPPORTED, "packed tensor: cooperative launch groups");
     HFG_CUDA(ctx, launch_eri_packed(L.la, L.lb, L.lc, L.ld, L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1],
                                     ctx->d_pairs.p, ctx->d_pairQ.p, thr, ctx->d_rec64.p, ctx->d_boys64.p, ctx->d_expt64.p, d_out,
                                     ctx->stream));

@@ -24,43 +24,13 @@
 #include <map>
 #include <vector>
 
+#include "df_handle.h"
 #include "df_internal.h"
 #include "df_umma.h"
 #include "hfg_ctx.h"
 
 using namespace hfg;
 
-struct hfg_df {
-  hfg_ctx* ctx = nullptr;
-  int n = 0, naux = 0, rank = 0;
-  long long ncol = 0;
-  int storage = HFG_DF_FP64;
-  DevBuf<double> B64;
-  DevBuf<float> B32;
-  DevBuf<__nv_bfloat16> B16;
-  DevBuf<int2> colmn;
-  DevBuf<double> metric;  // kept for inspection (naux x naux)
-  cublasHandle_t blas = nullptr;
-  DevBuf<double> P, pvec, gam, jcol, Cd, J, K, T64;
-  DevBuf<float> gam32, jcol32, pvec32, Kf, Tf, Cf;
-  DevBuf<__nv_bfloat16> Cb, Tb;
-  DevBuf<unsigned char> dense;
-  // tensor-core exchange: tile structure of the unpacked factor per operand
-  // type (built on first use) and its scratch
-  TileStructure tiles[2];
-  bool tiles_ready[2] = {false, false};
-  DevBuf<int> tile_off[2], tile_kt[2], tile_map[2];
-  UmmaWorkspace uws;
-  // device time of the last exchange (K) and its executed tensor-core flops
-  cudaEvent_t kev[2] = {nullptr, nullptr};
-  double k_flops = 0.0, tiles_fraction = 0.0;
-  bool k_timed = false;
-  ~hfg_df() {
-    for (auto& e : kev)
-      if (e) cudaEventDestroy(e);
-    if (blas) cublasDestroy(blas);
-  }
-};
 
 namespace {
 
@@ -462,10 +432,14 @@ namespace hfg {
 
 // J and K from occupied coefficients on the device: dC column-major n x nocc
 // (leading dimension n), i.e. the first nocc columns of an SCF C matrix.
-int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK, int mma) {
+int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK, int mma, int q_lo, int q_hi) {
   hfg_ctx* ctx = df->ctx;
   cudaStream_t st = ctx->stream;
-  const int n = df->n, rank = df->rank;
+  const int n = df->n;
+  // auxiliary functions [q_lo, q_hi) of the factor (a shard of the sum over Q)
+  if (q_hi < 0) q_hi = df->rank;
+  if (q_lo < 0 || q_lo > q_hi || q_hi > df->rank) return set_error(ctx, HFG_ERR_INVALID_INPUT, "auxiliary range");
+  const int rank = q_hi - q_lo;
   const long long ncol = df->ncol, nn = (long long)n * n;
   int rc = HFG_OK;
 #define CK(call)                         \
@@ -487,17 +461,23 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
     return set_error(ctx, HFG_ERR_CUDA, "P GEMM");
   // J: gamma = B p, j = B^T gamma (B row-major [rank][ncol] = column-major ncol x rank)
   CK(df->pvec.alloc(ncol));
-  CK(df->gam.alloc(rank));
+  CK(df->gam.alloc(std::max(rank, 1)));
   CK(df->jcol.alloc(ncol));
   CK(launch_pack_density(df->P.p, df->colmn.p, ncol, n, df->pvec.p, st));
   if (df->storage == HFG_DF_FP64) {
-    cublasDgemv(df->blas, CUBLAS_OP_T, (int)ncol, rank, &one, df->B64.p, (int)ncol, df->pvec.p, 1, &zero, df->gam.p, 1);
-    cublasDgemv(df->blas, CUBLAS_OP_N, (int)ncol, rank, &one, df->B64.p, (int)ncol, df->gam.p, 1, &zero, df->jcol.p, 1);
+    const double* Bq = df->B64.p + (size_t)q_lo * ncol;
+    if (rank > 0) {
+      cublasDgemv(df->blas, CUBLAS_OP_T, (int)ncol, rank, &one, Bq, (int)ncol, df->pvec.p, 1, &zero, df->gam.p, 1);
+      cublasDgemv(df->blas, CUBLAS_OP_N, (int)ncol, rank, &one, Bq, (int)ncol, df->gam.p, 1, &zero, df->jcol.p, 1);
+    } else {
+      CK(cudaMemsetAsync(df->jcol.p, 0, ncol * 8, st));
+    }
   } else {
     // the stored FP32 / BF16 factor with FP64 accumulation (J is
     // memory-bound; the density is not rounded)
     const bool bf = df->storage == HFG_DF_BF16;
-    CK(launch_df_j(bf ? 2 : 1, bf ? (const void*)df->B16.p : (const void*)df->B32.p, ncol, rank, df->pvec.p,
+    if (rank == 0) CK(cudaMemsetAsync(df->jcol.p, 0, ncol * 8, st));
+    CK(launch_df_j(bf ? 2 : 1, bf ? (const void*)(df->B16.p + (size_t)q_lo * ncol) : (const void*)(df->B32.p + (size_t)q_lo * ncol), ncol, rank, df->pvec.p,
                    df->gam.p, df->jcol.p, st));
   }
   CK(cudaMemsetAsync(dJ, 0, nn * 8, st));
@@ -517,6 +497,7 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
     ua.n = n;
     ua.nocc = nocc;
     ua.rank = rank;
+    ua.rank_offset = q_lo;
     ua.kind = kind;
     ua.storage = df->storage == HFG_DF_BF16 ? 2 : 1;
     ua.ncol = ncol;
@@ -554,13 +535,13 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   const size_t budget = std::max<size_t>((size_t)64 << 20, std::min<size_t>((size_t)4 << 30, free_b / 4));
-  int qc = (int)std::max<size_t>(1, std::min<size_t>((size_t)rank, budget / ((size_t)nn * esz)));
+  int qc = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(rank, 1), budget / ((size_t)nn * esz)));
   CK(df->dense.alloc((size_t)qc * nn * esz));
   CK(cudaMemsetAsync(dK, 0, nn * 8, st));
   if (mma == HFG_DF_FP64) {
     CK(df->T64.alloc((size_t)qc * n * nocc));
-    for (int q0 = 0; q0 < rank; q0 += qc) {
-      const int qn = std::min(qc, rank - q0);
+    for (int q0 = q_lo; q0 < q_hi; q0 += qc) {
+      const int qn = std::min(qc, q_hi - q0);
       CK(cudaMemsetAsync(df->dense.p, 0, (size_t)qn * nn * 8, st));
       // FP64 arithmetic on the stored factor, converted while unpacking
       const int um = df->storage == HFG_DF_FP64 ? 0 : (df->storage == HFG_DF_FP32 ? 3 : 4);
@@ -593,8 +574,8 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
     }
     const void* Bsrc = df->storage == HFG_DF_BF16 ? (const void*)df->B16.p : (const void*)df->B32.p;
     const int umode = df->storage == HFG_DF_BF16 ? 2 : (bf ? 5 : 1);
-    for (int q0 = 0; q0 < rank; q0 += qc) {
-      const int qn = std::min(qc, rank - q0);
+    for (int q0 = q_lo; q0 < q_hi; q0 += qc) {
+      const int qn = std::min(qc, q_hi - q0);
       CK(cudaMemsetAsync(df->dense.p, 0, (size_t)qn * nn * esz, st));
       CK(launch_df_unpack(umode, Bsrc, ncol, df->colmn.p, ncol, q0, qn, n, df->dense.p, st));
       rc = gemm_ex(ctx, df->blas, CUBLAS_OP_T, CUBLAS_OP_N, nocc, n * qn, n, Cin, it, n, df->dense.p, it, n, 0.0f,
@@ -618,9 +599,18 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
 
 }  // namespace hfg
 
-extern "C" int hfg_df_jk(hfg_df* df, const double* C_occ, int nocc, double* J, double* K, int mma) {
+namespace {
+
+// the shard's auxiliary functions: [shard * rank / nshards, (shard + 1) * rank / nshards)
+void shard_range(const hfg_df* df, int shard, int nshards, int& q_lo, int& q_hi) {
+  q_lo = (int)((long long)df->rank * shard / nshards);
+  q_hi = (int)((long long)df->rank * (shard + 1) / nshards);
+}
+
+int df_jk_host(hfg_df* df, const double* C_occ, int nocc, double* J, double* K, int mma, int shard, int nshards) {
   if (!df || !C_occ || !J || !K || nocc <= 0) return HFG_ERR_INVALID_INPUT;
   hfg_ctx* ctx = df->ctx;
+  if (nshards < 1 || shard < 0 || shard >= nshards) return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid shard");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
   AllocScope alloc_scope(ctx->stream);
@@ -634,9 +624,35 @@ extern "C" int hfg_df_jk(hfg_df* df, const double* C_occ, int nocc, double* J, d
   for (int i = 0; i < df->n; ++i)
     for (int k = 0; k < nocc; ++k) ct[(size_t)k * df->n + i] = C_occ[(size_t)i * nocc + k];
   cudaMemcpyAsync(df->Cd.p, ct.data(), ct.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
-  rc = df_jk_device(df, df->Cd.p, nocc, df->J.p, df->K.p, mma);
+  int q_lo, q_hi;
+  shard_range(df, shard, nshards, q_lo, q_hi);
+  rc = df_jk_device(df, df->Cd.p, nocc, df->J.p, df->K.p, mma, q_lo, q_hi);
   if (rc != HFG_OK) return rc;
   cudaMemcpyAsync(J, df->J.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream);
   cudaMemcpyAsync(K, df->K.p, nn * 8, cudaMemcpyDeviceToHost, ctx->stream);
   return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "df_jk sync");
+}
+
+}  // namespace
+
+extern "C" int hfg_df_jk(hfg_df* df, const double* C_occ, int nocc, double* J, double* K, int mma) {
+  return df_jk_host(df, C_occ, nocc, J, K, mma, 0, 1);
+}
+
+extern "C" int hfg_df_jk_shard(hfg_df* df, const double* C_occ, int nocc, double* J, double* K, int mma, int shard,
+                               int nshards) {
+  return df_jk_host(df, C_occ, nocc, J, K, mma, shard, nshards);
+}
+
+extern "C" int hfg_df_jk_device_shard(hfg_df* df, const double* d_C, int nocc, double* d_J, double* d_K, int mma,
+                                      int shard, int nshards) {
+  if (!df || !d_C || !d_J || !d_K || nocc <= 0) return HFG_ERR_INVALID_INPUT;
+  hfg_ctx* ctx = df->ctx;
+  if (nshards < 1 || shard < 0 || shard >= nshards) return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid shard");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  AllocScope alloc_scope(ctx->stream);
+  int q_lo, q_hi;
+  shard_range(df, shard, nshards, q_lo, q_hi);
+  return df_jk_device(df, d_C, nocc, d_J, d_K, mma, q_lo, q_hi);
 }

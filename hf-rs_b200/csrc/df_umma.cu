@@ -35,6 +35,8 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -189,19 +191,32 @@ __device__ __forceinline__ uint32_t make_idesc(uint32_t fmt, uint32_t M, uint32_
   return (1u << 4) | (fmt << 7) | (fmt << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // ----------------------------------------------------------------- kernel --
+// Persistent: one block per SM walks the launch's work units (output tiles,
+// or output tile x Q range for the symmetric update) with a grid stride.
+// The shared-memory ring runs continuously across units, and the TMEM
+// accumulator is double-buffered (2 x 256 columns), so the epilogue of one
+// unit overlaps the main loop of the next.
 struct GemmArgs {
-  int mode;            // 0: T_Q = B_Q C over non-zero tiles; 1: K_lower += T T^T
-  int m_rows;          // valid rows of the output (n)
-  int n_cols;          // valid columns of the output (mode 0: nocc_pad; mode 1: n)
-  // mode 0
+  int mode;    // 0: T_Q = B_Q C over non-zero tiles; 1: K_lower += T T^T
+  int m_rows;  // valid rows of the output (n)
+  int n_cols;  // valid columns of the output (mode 0: nocc_pad; mode 1: n)
+  int bn;      // output tile width (<= 256, multiple of 16)
+  long long units;  // work units of the launch
+  // mode 0: unit = (nt, mt, Q), nt fastest
   const int* tile_off;  // per row block: its non-zero tiles [tile_off[mt], tile_off[mt + 1])
   const int* tile_kt;   // column block of each non-zero tile (tiles numbered in row-block order)
-  // mode 1
+  int n_ntiles, n_mtiles;
+  // mode 1: unit = (lower tile, Q range), lower tile fastest
   const int2* out_tiles;  // (mt, nt) of every lower output tile
-  int q_count;            // Q of the chunk
+  int n_lower;
+  int q_count;  // Q of the chunk
   int q_per_split;
-  int i_tiles;            // K tiles per Q (ceil(nocc_pad / BK))
+  int i_tiles;  // K tiles per Q (ceil(nocc_pad / BK))
   // output
   void* out;
   long long ldo;           // row stride (elements)
@@ -209,56 +224,72 @@ struct GemmArgs {
   int* err;
 };
 
+struct Unit {
+  int mt, nt, q, q0, nk;
+};
+
+template <int MODE>
+__device__ __forceinline__ Unit unit_of(const GemmArgs& a, long long u) {
+  Unit w;
+  if (MODE == 0) {
+    w.nt = (int)(u % a.n_ntiles);
+    const long long r = u / a.n_ntiles;
+    w.mt = (int)(r % a.n_mtiles);
+    w.q = (int)(r / a.n_mtiles);
+    w.q0 = 0;
+    w.nk = __ldg(a.tile_off + w.mt + 1) - __ldg(a.tile_off + w.mt);
+  } else {
+    const int t = (int)(u % a.n_lower), sp = (int)(u / a.n_lower);
+    const int2 tt = a.out_tiles[t];
+    w.mt = tt.x;
+    w.nt = tt.y;
+    w.q = 0;
+    w.q0 = sp * a.q_per_split;
+    const int q1 = min(a.q_count, w.q0 + a.q_per_split);
+    w.nk = q1 > w.q0 ? (q1 - w.q0) * a.i_tiles : 0;
+  }
+  return w;
+}
+
+// MMA N of a unit: its output columns rounded up to 16 (columns past
+// n_cols read zero-filled rows of B and are not stored)
+__device__ __forceinline__ int unit_cols(const GemmArgs& a, const Unit& w) {
+  return (min(a.bn, a.n_cols - w.nt * a.bn) + 15) & ~15;
+}
+
 template <int KIND, int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const GemmArgs a) {
   constexpr uint32_t kFmt = KIND == kBF16 ? 1u : 2u;
-  constexpr int kEl = KIND == kBF16 ? 2 : 4;  // operand bytes
-  constexpr int kKPerMma = 32 / kEl;          // 16 (BF16) or 8 (TF32): 32 bytes of K per instruction
-  (void)kKPerMma;
+  constexpr int kEl = KIND == kBF16 ? 2 : 4;  // operand bytes; 32 bytes of K per instruction
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* sA = base;
   unsigned char* sB = base + kStages * kStageA;
   uint64_t* full = (uint64_t*)(sB + kStages * kStageB);
   uint64_t* empty = full + kStages;
-  uint64_t* accum = empty + kStages;
-  uint32_t* tmem_slot = (uint32_t*)(accum + 1);
+  uint64_t* tfull = empty + kStages;  // accumulator buffer b holds a finished unit
+  uint64_t* tempty = tfull + 2;       // accumulator buffer b has been read out
+  uint64_t* done = tempty + 2;
+  uint32_t* tmem_slot = (uint32_t*)(done + 1);
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  // ---- this block's output tile and K range
-  int mt, nt, nk, q0 = 0;
-  if (MODE == 0) {
-    nt = blockIdx.x;
-    mt = blockIdx.y;
-    nk = a.tile_off[mt + 1] - a.tile_off[mt];
-  } else {
-    const int2 t = a.out_tiles[blockIdx.x];
-    mt = t.x;
-    nt = t.y;
-    q0 = blockIdx.y * a.q_per_split;
-    const int q1 = min(a.q_count, q0 + a.q_per_split);
-    nk = q1 > q0 ? (q1 - q0) * a.i_tiles : 0;
-  }
-  const int m0 = mt * kBM, n0 = nt * kBN;
-  // columns of this output tile: the MMA's N is a multiple of 16 (columns
-  // past n_cols read zero-filled rows of B and are not stored)
-  const int ncols = (min(kBN, a.n_cols - n0) + 15) & ~15;
-  const int Q = MODE == 0 ? (int)blockIdx.z : 0;
-
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accum, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
+    }
+    mbar_init(done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
-    tmem_alloc(tmem_slot, kTmemCols);
+    tmem_alloc(tmem_slot, 2 * kTmemCols);
     tmem_relinquish();
   }
   tc_fence_before();
@@ -266,85 +297,112 @@ __global__ void __launch_bounds__(kThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 0 && lane == 0 && nk > 0) {
+  if (warp == 0 && lane == 0) {
     // ---------------------------------------------------------- producer
-    int issued[kStages];
+    int last_round[kStages];
 #pragma unroll
-    for (int s = 0; s < kStages; ++s) issued[s] = 0;
+    for (int s = 0; s < kStages; ++s) last_round[s] = -1;
     const uint32_t bytes = (uint32_t)(kStageA + kStageB);
-    for (int it = 0; it < nk; ++it) {
-      const int s = it % kStages;
-      const uint32_t round = (uint32_t)(it / kStages);
-      if (!mbar_wait(&empty[s], (round & 1u) ^ 1u, abort_flag)) {
-        if (!*abort_flag) atomicExch(a.err, 1);
-        *abort_flag = 1;
-        break;
+    long long it = 0;
+    for (long long u = blockIdx.x; u < a.units && !*abort_flag; u += gridDim.x) {
+      const Unit w = unit_of<MODE>(a, u);
+      for (int k = 0; k < w.nk; ++k, ++it) {
+        const int s = (int)(it % kStages);
+        const uint32_t round = (uint32_t)(it / kStages);
+        if (!mbar_wait(&empty[s], (round & 1u) ^ 1u, abort_flag)) {
+          if (!*abort_flag) atomicExch(a.err, 1);
+          *abort_flag = 1;
+          break;
+        }
+        mbar_expect_tx(&full[s], bytes);
+        int ax, ay, az, bx, by, bz;
+        if (MODE == 0) {
+          const int t = __ldg(a.tile_off + w.mt) + k;
+          ax = 0;
+          ay = t * kBM;
+          az = w.q;
+          bx = __ldg(a.tile_kt + t) * (kRowBytes / kEl);
+          by = w.nt * a.bn;
+          bz = 0;
+        } else {
+          const int q = w.q0 + k / a.i_tiles, ib = k % a.i_tiles;
+          ax = bx = ib * (kRowBytes / kEl);
+          ay = w.mt * kBM;
+          by = w.nt * a.bn;
+          az = bz = q;
+        }
+        tma_load_3d(sA + s * kStageA, &tmA, &full[s], ax, ay, az);
+        tma_load_3d(sB + s * kStageB, &tmB, &full[s], bx, by, bz);
+        last_round[s] = (int)round;
       }
-      mbar_expect_tx(&full[s], bytes);
-      int ax, ay, az, bx, by, bz;
-      if (MODE == 0) {
-        const int t = a.tile_off[mt] + it;
-        ax = 0;
-        ay = t * kBM;
-        az = Q;
-        bx = a.tile_kt[t] * (kRowBytes / kEl);
-        by = n0;
-        bz = 0;
-      } else {
-        const int q = q0 + it / a.i_tiles, ib = it % a.i_tiles;
-        ax = bx = ib * (kRowBytes / kEl);
-        ay = m0;
-        by = n0;
-        az = bz = q;
-      }
-      tma_load_3d(sA + s * kStageA, &tmA, &full[s], ax, ay, az);
-      tma_load_3d(sB + s * kStageB, &tmB, &full[s], bx, by, bz);
-      ++issued[s];
     }
     // let every copy this thread issued land before the block may exit
     for (int s = 0; s < kStages; ++s)
-      if (issued[s] > 0 && !mbar_wait_drain(&full[s], (uint32_t)((issued[s] - 1) & 1))) atomicExch(a.err, 2);
-  } else if (warp == 1 && lane == 0 && nk > 0) {
+      if (last_round[s] >= 0 && !mbar_wait_drain(&full[s], (uint32_t)(last_round[s] & 1))) atomicExch(a.err, 2);
+  } else if (warp == 1 && lane == 0) {
     // ------------------------------------------------------- MMA issuer
-    const uint32_t idesc = make_idesc(kFmt, kBM, (uint32_t)ncols);
-    for (int it = 0; it < nk; ++it) {
-      const int s = it % kStages;
-      const uint32_t round = (uint32_t)(it / kStages);
-      if (!mbar_wait(&full[s], round & 1u, abort_flag)) {
+    long long it = 0;
+    int lt = 0;
+    for (long long u = blockIdx.x; u < a.units && !*abort_flag; u += gridDim.x, ++lt) {
+      const Unit w = unit_of<MODE>(a, u);
+      const int b = lt & 1;
+      const uint32_t use = (uint32_t)(lt >> 1);
+      if (!mbar_wait(&tempty[b], (use & 1u) ^ 1u, abort_flag)) {
         if (!*abort_flag) atomicExch(a.err, 3);
         *abort_flag = 1;
         break;
       }
       tc_fence_after();
-      const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sB + s * kStageB);
+      const uint32_t d = tmem + (uint32_t)(b * kTmemCols);
+      const uint32_t idesc = make_idesc(kFmt, kBM, (uint32_t)unit_cols(a, w));
+      bool ok = true;
+      for (int k = 0; k < w.nk; ++k, ++it) {
+        const int s = (int)(it % kStages);
+        const uint32_t round = (uint32_t)(it / kStages);
+        if (!mbar_wait(&full[s], round & 1u, abort_flag)) {
+          if (!*abort_flag) atomicExch(a.err, 4);
+          *abort_flag = 1;
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sB + s * kStageB);
 #pragma unroll
-      for (int k = 0; k < 4; ++k)  // 4 x 32 bytes of K per 128-byte row
-        umma<KIND>(tmem, sw128_desc(a0 + 32 * k), sw128_desc(b0 + 32 * k), idesc, (it > 0 || k > 0) ? 1u : 0u);
-      umma_commit(&empty[s]);  // the slot is free once these MMAs have read it
+        for (int kk = 0; kk < 4; ++kk)  // 4 x 32 bytes of K per 128-byte row
+          umma<KIND>(d, sw128_desc(a0 + 32 * kk), sw128_desc(b0 + 32 * kk), idesc, (k > 0 || kk > 0) ? 1u : 0u);
+        umma_commit(&empty[s]);  // the slot is free once these MMAs have read it
+      }
+      if (!ok) break;
+      umma_commit(&tfull[b]);  // with no MMAs (nk = 0) it arrives at once
     }
-    umma_commit(accum);  // always: completes when every MMA issued above is done
+    // every MMA issued above completes before TMEM is freed
+    umma_commit(done);
+    if (!mbar_wait_drain(done, 0u)) atomicExch(a.err, 5);
   } else if (warp >= 2) {
     // --------------------------------------------------------- epilogue
     const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31 belong to this warp
-    const int row = m0 + quarter * 32 + lane;
-    bool ok = true;
-    if (nk > 0) {
-      ok = mbar_wait(accum, 0u, abort_flag);
+    int lt = 0;
+    for (long long u = blockIdx.x; u < a.units; u += gridDim.x, ++lt) {
+      const Unit w = unit_of<MODE>(a, u);
+      const int b = lt & 1;
+      const uint32_t use = (uint32_t)(lt >> 1);
+      bool ok = mbar_wait(&tfull[b], use & 1u, abort_flag);
+      // tcgen05.ld is warp-collective: the whole warp reads or none of it
+      ok = __all_sync(0xffffffffu, ok);
       if (!ok) {
-        if (!*abort_flag) atomicExch(a.err, 4);
-        *abort_flag = 1;
-        // the MMA issuer always commits to `accum`: wait for its work to end
-        mbar_wait_drain(accum, 0u);
+        if (lane == 0) {
+          if (!*abort_flag) atomicExch(a.err, 6);
+          *abort_flag = 1;
+        }
+        break;
       }
       tc_fence_after();
-    }
-    // tcgen05.ld is warp-collective: the whole warp reads or none of it
-    ok = __all_sync(0xffffffffu, ok);
-    if (ok) {
-      const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
+      const int row = w.mt * kBM + quarter * 32 + lane;
+      const int n0 = w.nt * a.bn, ncols = unit_cols(a, w);
+      const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * kTmemCols);
       for (int c = 0; c < ncols; c += 16) {
         float v[16];
-        if (nk > 0) {
+        if (w.nk > 0) {
           tmem_ld16(lane_addr + (uint32_t)c, v);
         } else {
 #pragma unroll
@@ -352,16 +410,16 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         if (row >= a.m_rows) continue;
         if (MODE == 0) {
-          // n_cols (nocc_pad) and every tile's width are multiples of 16
-          const long long off = (long long)Q * a.batch_stride + (long long)row * a.ldo + n0 + c;
+          // n_cols (nocc_pad) and every unit's width are multiples of 16
+          const long long off = (long long)w.q * a.batch_stride + (long long)row * a.ldo + n0 + c;
           if (KIND == kBF16) {
             __nv_bfloat16* o = (__nv_bfloat16*)a.out + off;
-            uint4 w[2];
-            __nv_bfloat162* h = (__nv_bfloat162*)w;
+            uint4 q4[2];
+            __nv_bfloat162* h = (__nv_bfloat162*)q4;
 #pragma unroll
             for (int k = 0; k < 8; ++k) h[k] = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
-            ((uint4*)o)[0] = w[0];
-            ((uint4*)o)[1] = w[1];
+            ((uint4*)o)[0] = q4[0];
+            ((uint4*)o)[1] = q4[1];
           } else {
             float4* o = (float4*)((float*)a.out + off);
 #pragma unroll
@@ -376,13 +434,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (n0 + c + k < a.n_cols) atomicAdd(o + k, v[k]);
         }
       }
+      // hand the buffer back to the MMA issuer once this warp's reads are done
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem, kTmemCols);
+    tmem_dealloc(tmem, 2 * kTmemCols);
   }
 }
 
@@ -571,6 +633,7 @@ cudaError_t df_k_tensor_cores(const UmmaDfArgs& p, UmmaWorkspace& ws, int* statu
   // executed MMA work: GEMM 1 over the non-zero tiles of every row block,
   // GEMM 2 over the lower output tiles (N of the edge tiles as issued)
   {
+    // (the column tiles' widths sum to nocc_pad)
     double f1 = 2.0 * kBM * tk * (double)ts.ntiles * nocc_pad;
     double f2 = 0.0;
     for (const int2& t : lower) f2 += 2.0 * kBM * (double)((std::min(kBN, n - t.y * kBN) + 15) / 16 * 16);
@@ -578,8 +641,15 @@ cudaError_t df_k_tensor_cores(const UmmaDfArgs& p, UmmaWorkspace& ws, int* statu
     ws.flops_executed = (f1 + f2) * p.rank;
     ws.tiles_fraction = ts.total_tiles > 0 ? (double)ts.ntiles / ts.total_tiles : 0.0;
   }
+  // HFG_PROFILE=1: device time of each phase, summed over the chunks, on stderr
+  static const bool profile = getenv("HFG_PROFILE") && getenv("HFG_PROFILE")[0] == '1';
+  cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr};
+  float pms[3] = {0.f, 0.f, 0.f};
+  if (profile)
+    for (auto& x : pev) cudaEventCreate(&x);
   for (int q0 = 0; q0 < p.rank; q0 += qc) {
     const int qn = std::min(qc, p.rank - q0);
+    if (profile) cudaEventRecord(pev[0], st);
     // 1. unpack the chunk's non-zero tiles
     {
       dim3 g((unsigned)ts.ntiles, (unsigned)std::min(qn, 64));
@@ -599,6 +669,7 @@ cudaError_t df_k_tensor_cores(const UmmaDfArgs& p, UmmaWorkspace& ws, int* statu
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
     }
+    if (profile) cudaEventRecord(pev[1], st);
     // 2. T_Q = B_Q C: A = tile-compact chunk (x: tk, y: tile rows, z: Q)
     if (!make_map(&mA1, kind, ws.dense.p, tk, (long long)ts.ntiles * kBM, qn, (long long)tk * el,
                   (long long)ts.ntiles * kBM * tk * el, kBM))
@@ -613,32 +684,58 @@ cudaError_t df_k_tensor_cores(const UmmaDfArgs& p, UmmaWorkspace& ws, int* statu
     g1.ldo = nocc_pad;
     g1.batch_stride = (long long)n * nocc_pad;
     g1.err = (int*)ws.err.p;
-    dim3 grid1((unsigned)((nocc_pad + kBN - 1) / kBN), (unsigned)nmt, (unsigned)qn);
+    // equal column tiles of at most 256 (a narrow remainder tile would run
+    // the tensor cores below their rate)
+    g1.n_ntiles = (nocc_pad + kBN - 1) / kBN;
+    g1.bn = ((nocc_pad + g1.n_ntiles - 1) / g1.n_ntiles + 15) / 16 * 16;
+    g1.n_mtiles = nmt;
+    g1.units = (long long)g1.n_ntiles * nmt * qn;
+    dim3 grid1((unsigned)std::min<long long>(g1.units, sms));
     e = kind == kBF16 ? launch_gemm<kBF16, 0>(mA1, mCt, g1, grid1, st) : launch_gemm<kTF32, 0>(mA1, mCt, g1, grid1, st);
     if (e != cudaSuccess) return e;
+    if (profile) cudaEventRecord(pev[2], st);
     // 3. K_lower += T T^T over this chunk's Q, split so that the grid covers
     //    the SMs a few times
     if (!make_map(&mT_A, kind, ws.T.p, nocc_pad, n, qn, (long long)nocc_pad * el, (long long)n * nocc_pad * el, kBM) ||
         !make_map(&mT_B, kind, ws.T.p, nocc_pad, n, qn, (long long)nocc_pad * el, (long long)n * nocc_pad * el, kBN))
       return cudaErrorInvalidValue;
-    int splits = std::max(1, std::min(qn, (4 * sms + (int)lower.size() - 1) / (int)lower.size()));
+    // work units: (lower tile, Q range), about eight per SM for balance
+    int splits = std::max(1, std::min(qn, (8 * sms + (int)lower.size() - 1) / (int)lower.size()));
     const int qps = (qn + splits - 1) / splits;
     splits = (qn + qps - 1) / qps;
     GemmArgs g2{};
     g2.mode = 1;
     g2.m_rows = n;
     g2.n_cols = n;
+    g2.bn = kBN;
     g2.out_tiles = (const int2*)ws.lower.p;
+    g2.n_lower = (int)lower.size();
     g2.q_count = qn;
     g2.q_per_split = qps;
     g2.i_tiles = i_tiles;
+    g2.units = (long long)lower.size() * splits;
     g2.out = ws.Kf.p;
     g2.ldo = n;
     g2.err = (int*)ws.err.p;
-    dim3 grid2((unsigned)lower.size(), (unsigned)splits);
+    dim3 grid2((unsigned)std::min<long long>(g2.units, sms));
     e = kind == kBF16 ? launch_gemm<kBF16, 1>(mT_A, mT_B, g2, grid2, st)
                       : launch_gemm<kTF32, 1>(mT_A, mT_B, g2, grid2, st);
     if (e != cudaSuccess) return e;
+    if (profile) {
+      cudaEventRecord(pev[3], st);
+      cudaEventSynchronize(pev[3]);
+      for (int k = 0; k < 3; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, pev[k], pev[k + 1]);
+        pms[k] += ms;
+      }
+    }
+  }
+  if (profile) {
+    fprintf(stderr, "hfg-profile df-exchange %s n %d nocc %d rank %d chunk %d tiles %d/%d: unpack %.3f ms, "
+                    "T = B C %.3f ms, K += T T^T %.3f ms\n",
+            kind == kBF16 ? "bf16" : "tf32", n, nocc, p.rank, qc, ts.ntiles, ts.total_tiles, pms[0], pms[1], pms[2]);
+    for (auto& x : pev) cudaEventDestroy(x);
   }
   {
     const long long tot = (long long)n * n;

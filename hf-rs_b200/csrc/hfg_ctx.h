@@ -34,7 +34,7 @@ struct PairClass {
 };
 
 struct Launch {
-  int la, lb, lc, ld, G;
+  int la, lb, lc, ld;
   cudaStream_t st = nullptr;  // stream of the entries/prefix allocations
   bool fp32;
   double quartets = 0, prims = 0;  // shell quartets and primitive quartets (after screening) of this launch
@@ -142,8 +142,11 @@ struct hfg_ctx {
 struct hfg_df;
 
 namespace hfg {
-// Implemented in df.cu: DF J/K from column-major occupied coefficients.
-int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK, int mma);
+// Implemented in df.cu: DF J/K from column-major occupied coefficients,
+// summed over the auxiliary functions [q_lo, q_hi) of the factor (q_hi < 0:
+// all of them).
+int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK, int mma, int q_lo = 0,
+                 int q_hi = -1);
 // Implemented in ctx.cu, used by scf.cu.
 // shard / nshards: only the shard's cost-balanced range of work-queue steps
 // of every launch (the partial J/K of all shards sum to the full build)

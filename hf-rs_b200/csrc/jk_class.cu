@@ -14,13 +14,13 @@ namespace hfg {
 
 // Persistent grid: as many resident blocks as the kernel's occupancy allows
 // on every SM, capped by the work.
-template <typename T, int NS, int G>
+template <typename T, int NS>
 static cudaError_t launch_t(const JKLaunchArgs& a, cudaStream_t st) {
   constexpr int L = EriClass<HFG_LA, HFG_LB, HFG_LC, HFG_LD>::L;
   constexpr int block = 256;
   (void)L;
   const size_t smem = boys_smem_bytes<T>();
-  auto kern = jk_kernel<HFG_LA, HFG_LB, HFG_LC, HFG_LD, T, NS, G>;
+  auto kern = jk_kernel<HFG_LA, HFG_LB, HFG_LC, HFG_LD, T, NS>;
   // resident blocks per device (a process may drive different device
   // models), looked up once per device
   constexpr int kMaxDev = 64;
@@ -45,20 +45,9 @@ static cudaError_t launch_t(const JKLaunchArgs& a, cudaStream_t st) {
 
 #define HFG_CAT2(a, b, c, d) launch_jk_##a##b##c##d
 #define HFG_CAT(a, b, c, d) HFG_CAT2(a, b, c, d)
-template <int G>
-static cudaError_t launch_g(const JKLaunchArgs& a, bool fp32, cudaStream_t st) {
-  if (a.nspin == 2) return fp32 ? launch_t<float, 2, G>(a, st) : launch_t<double, 2, G>(a, st);
-  return fp32 ? launch_t<float, 1, G>(a, st) : launch_t<double, 1, G>(a, st);
-}
-
-cudaError_t HFG_CAT(HFG_LA, HFG_LB, HFG_LC, HFG_LD)(const JKLaunchArgs& a, int G, bool fp32, cudaStream_t st) {
-  constexpr int nacc = EriClass<HFG_LA, HFG_LB, HFG_LC, HFG_LD>::NACC;
-  if constexpr (nacc <= kMaxAccCoop) {
-    if (G == 8) return launch_g<8>(a, fp32, st);
-    if (G == 32) return launch_g<32>(a, fp32, st);
-  }
-  if (G != 1) return cudaErrorInvalidValue;
-  return launch_g<1>(a, fp32, st);
+cudaError_t HFG_CAT(HFG_LA, HFG_LB, HFG_LC, HFG_LD)(const JKLaunchArgs& a, bool fp32, cudaStream_t st) {
+  if (a.nspin == 2) return fp32 ? launch_t<float, 2>(a, st) : launch_t<double, 2>(a, st);
+  return fp32 ? launch_t<float, 1>(a, st) : launch_t<double, 1>(a, st);
 }
 
 }  // namespace hfg

@@ -4,9 +4,9 @@
 
 namespace hfg {
 
-cudaError_t launch_jk(int la, int lb, int lc, int ld, int G, bool fp32, const JKLaunchArgs& a, cudaStream_t st) {
+cudaError_t launch_jk(int la, int lb, int lc, int ld, bool fp32, const JKLaunchArgs& a, cudaStream_t st) {
 #define HFG_CASE(A, B, C, D) \
-  if (la == A && lb == B && lc == C && ld == D) return launch_jk_##A##B##C##D(a, G, fp32, st);
+  if (la == A && lb == B && lc == C && ld == D) return launch_jk_##A##B##C##D(a, fp32, st);
   HFG_CASE(0, 0, 0, 0)
   HFG_CASE(1, 0, 0, 0)
   HFG_CASE(1, 0, 1, 0)

@@ -80,11 +80,14 @@ struct DBlocks {
 
 // Fused digestion of one scaled Cartesian block (w already includes deg and
 // the component scales), except J'[a,b] which the caller reduces across the
-// warp (jab receives this lane's sum over c,d).
-template <int LA, int LB, int LC, int LD, int NS, typename DT>
+// warp (jab receives this lane's sum over c,d).  With SEG, K'[a,c] and
+// K'[b,c] are returned in kac / kbc for the caller's segmented reduction
+// over lanes that share shell c, instead of being added here.
+template <int LA, int LB, int LC, int LD, int NS, typename DT, bool SEG>
 __device__ __forceinline__ void digest(const DT* __restrict__ w, const PairInfo& bra, const PairInfo& ket,
                                        const JKLaunchArgs& a, const DBlocks<LA, LB, LC, LD, NS, DT>& d,
-                                       DT* __restrict__ jab) {
+                                       DT* __restrict__ jab, DT (*__restrict__ kac)[ncart(LA) * ncart(LC)],
+                                       DT (*__restrict__ kbc)[ncart(LB) * ncart(LC)]) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   const int n = a.n;
   const int i0 = bra.ao_a, j0 = bra.ao_b, k0 = ket.ao_a, l0 = ket.ao_b;
@@ -116,7 +119,8 @@ __device__ __forceinline__ void digest(const DT* __restrict__ w, const PairInfo&
         for (int j = 0; j < NB; ++j)
 #pragma unroll
           for (int l = 0; l < ND; ++l) s += w[((i * NB + j) * NC + k) * ND + l] * d.bd[sp][j * ND + l];
-        atomicAdd(K + (size_t)(i0 + i) * n + k0 + k, 2.0 * (double)s);
+        if (SEG) kac[sp][i * NC + k] = s;
+        else atomicAdd(K + (size_t)(i0 + i) * n + k0 + k, 2.0 * (double)s);
       }
 #pragma unroll
     for (int j = 0; j < NB; ++j)
@@ -127,7 +131,8 @@ __device__ __forceinline__ void digest(const DT* __restrict__ w, const PairInfo&
         for (int i = 0; i < NA; ++i)
 #pragma unroll
           for (int l = 0; l < ND; ++l) s += w[((i * NB + j) * NC + k) * ND + l] * d.ad[sp][i * ND + l];
-        atomicAdd(K + (size_t)(j0 + j) * n + k0 + k, 2.0 * (double)s);
+        if (SEG) kbc[sp][j * NC + k] = s;
+        else atomicAdd(K + (size_t)(j0 + j) * n + k0 + k, 2.0 * (double)s);
       }
 #pragma unroll
     for (int i = 0; i < NA; ++i)
@@ -180,36 +185,45 @@ template <int LA, int LB, int LC, int LD, typename T> struct MinBlocks {
   static constexpr int value = sizeof(T) == 4 ? f32 : f64;
 };
 
-// 1: the digestion's density blocks are loaded before the primitive loop
-// (their latency overlaps the integral work, at the cost of registers held
-// through the loop); 0: after it (measured faster on every hot class).
-#ifndef HFG_JK_HOIST_D
-#define HFG_JK_HOIST_D 0
-#endif
-
 // 1: start fetching the next task's ket pair and primitive records while
 // this task computes.
 #ifndef HFG_JK_PREFETCH
 #define HFG_JK_PREFETCH 1
 #endif
-// 1: the ket primitive pairs that survive against the largest bra one are
-// counted by a binary search before the loop; 0: tested inside the loop.
-#ifndef HFG_JK_NKE_SEARCH
-#define HFG_JK_NKE_SEARCH 0
-#endif
-
 // Bring the 128-byte line holding p into L1 without waiting for it.
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
-// G lanes per shell quartet (G = 1: one quartet per lane).  With G > 1 the
-// lanes of a group take the quartet's ket primitive pairs round-robin (they
-// are sorted by bound, so neighbouring lanes see similar screening), all
-// walk the shared bra primitive pairs, and the group reduces its
-// accumulators with shuffles before one lane digests the block.
-template <int LA, int LB, int LC, int LD, typename T, int NS, int G>
+
+// K'[a,c], K'[b,c] of FP32 launches are summed over the lanes that share the
+// ket's first shell c before their atomics (kets are ordered by AO index
+// within each Schwarz bucket, so such lanes are neighbours); FP64 launches
+// add them per lane.  HFG_JK_SEG_F64=1 / HFG_JK_SEG_F32=0 override this in
+// tuning builds.
+#ifndef HFG_JK_SEG_F64
+#define HFG_JK_SEG_F64 0
+#endif
+#ifndef HFG_JK_SEG_F32
+#define HFG_JK_SEG_F32 1
+#endif
+
+// Sum of v over this lane's run of lanes [lane, end), left in the run's
+// first lane (segmented tree over contiguous runs of at most 32 lanes).
+template <typename T>
+__device__ __forceinline__ T run_sum(T v, int lane, int end) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T o = __shfl_down_sync(0xffffffffu, v, off);
+    if (lane + off < end) v += o;
+  }
+  return v;
+}
+
+// A warp takes one bra shell pair and up to 32 ket pairs of one pair class,
+// one shell quartet per lane.
+template <int LA, int LB, int LC, int LD, typename T, int NS>
 __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk_kernel(const JKLaunchArgs a) {
-  constexpr int QPW = 32 / G;
   using C = EriClass<LA, LB, LC, LD>;
+  constexpr bool SEG = sizeof(T) == 4 ? HFG_JK_SEG_F32 : HFG_JK_SEG_F64;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
@@ -234,27 +248,22 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
         next = a.prefix[e + 1];
       }
       const JKEntry ent = a.entries[e];
-      const int grp = lane / G, gl = lane - grp * G;
-      const int kidx = ent.k_lo + (int)(warp - a.prefix[e]) * QPW + grp;
+      const int kidx = ent.k_lo + (int)(warp - a.prefix[e]) * 32 + lane;
       // kets are bucketed by bound: the exact Schwarz test per quartet
       const bool active = kidx < ent.k_hi && __ldg(a.pairQ + kidx) * __ldg(a.pairQ + ent.bra) > a.thr;
       const PairInfo bra = a.pairs[ent.bra];
       const PairInfo ket = a.pairs[active ? kidx : ent.k_lo];
       // the next task usually continues this entry: start fetching its ket
       // pair, and its first primitive records (kets of one class have equal
-      // primitive counts and consecutive records, so they start QPW * npp on)
-      if (HFG_JK_PREFETCH && warp + 1 < t1 && kidx + QPW < ent.k_hi) {
-        prefetch_l1(&a.pairs[kidx + QPW]);
-        prefetch_l1(RecOf<T>::get(a) + ket.rec_off + QPW);
-        prefetch_l1(a.pbound + ket.rec_off + QPW);
+      // primitive counts and consecutive records, so they start 32 on)
+      if (HFG_JK_PREFETCH && warp + 1 < t1 && kidx + 32 < ent.k_hi) {
+        prefetch_l1(&a.pairs[kidx + 32]);
+        prefetch_l1(RecOf<T>::get(a) + ket.rec_off + 32);
+        prefetch_l1(a.pbound + ket.rec_off + 32);
       }
-      DBlocks<LA, LB, LC, LD, NS, T> dblk;
-      if (HFG_JK_HOIST_D && active && gl == 0) dblk.load(bra, ket, a);
-
       T acc[C::NACC];
 #pragma unroll
       for (int x = 0; x < C::NACC; ++x) acc[x] = (T)0;
-
       if (active) {
         using Rec = typename RecOf<T>::type;
         const T ACx = (T)(bra.Ax - ket.Ax), ACy = (T)(bra.Ay - ket.Ay), ACz = (T)(bra.Az - ket.Az);
@@ -272,23 +281,15 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
         // ket primitive pairs while they survive against the largest bra one
         // (bounds sorted descending); the next record and bound are fetched
         // one iteration ahead
-        int nke = nk;
-        if (HFG_JK_NKE_SEARCH) {
-          int lo = 0;
-          while (lo < nke) {
-            const int mid = (lo + nke) >> 1;
-            if (kb[mid * ks] * bmax >= eps) lo = mid + 1; else nke = mid;
-          }
-        }
-        Rec Qn = kr[(gl < nk ? gl : 0) * ks];
-        float qbn = kb[(gl < nk ? gl : 0) * ks];
-        for (int ik = gl; ik < nke; ik += G) {
+        Rec Qn = kr[0];
+        float qbn = kb[0];
+        for (int ik = 0; ik < nk; ++ik) {
           const Rec Q = Qn;
           const float qb = qbn;
-          if (!HFG_JK_NKE_SEARCH && qb * bmax < eps) break;
-          if (ik + G < nke) {
-            Qn = kr[(ik + G) * ks];
-            qbn = kb[(ik + G) * ks];
+          if (qb * bmax < eps) break;
+          if (ik + 1 < nk) {
+            Qn = kr[(ik + 1) * ks];
+            qbn = kb[(ik + 1) * ks];
           }
           const T QCx = -Q.bp * kABx, QCy = -Q.bp * kABy, QCz = -Q.bp * kABz;
           int ib = 0;
@@ -314,16 +315,11 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
           }
         }
       }
-      if (G > 1) {
-#pragma unroll
-        for (int x = 0; x < C::NACC; ++x) {
-#pragma unroll
-          for (int off = G / 2; off > 0; off >>= 1) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], off);
-        }
-      }
       T jab[NAB];
-      if (active && gl == 0) {
-        if (!HFG_JK_HOIST_D) dblk.load(bra, ket, a);
+      T kac[NS][NA * NC], kbc[NS][NB * NC];
+      if (active) {
+        DBlocks<LA, LB, LC, LD, NS, T> dblk;
+        dblk.load(bra, ket, a);
         T out[C::NOUT];
         C::hrr(acc, out, (T)bra.ABx, (T)bra.ABy, (T)bra.ABz, (T)ket.ABx, (T)ket.ABy, (T)ket.ABz);
         T deg = (T)1;
@@ -343,10 +339,48 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
                 const int x = ((i * NB + j) * NC + k) * ND + l;
                 out[x] *= deg * (T)(comp_scale(LA, i) * comp_scale(LB, j) * comp_scale(LC, k) * comp_scale(LD, l));
               }
-        digest<LA, LB, LC, LD, NS, T>(out, bra, ket, a, dblk, jab);
+        digest<LA, LB, LC, LD, NS, T, SEG>(out, bra, ket, a, dblk, jab, kac, kbc);
       } else {
 #pragma unroll
         for (int x = 0; x < NAB; ++x) jab[x] = (T)0;
+        if (SEG) {
+#pragma unroll
+          for (int sp = 0; sp < NS; ++sp) {
+#pragma unroll
+            for (int x = 0; x < NA * NC; ++x) kac[sp][x] = (T)0;
+#pragma unroll
+            for (int x = 0; x < NB * NC; ++x) kbc[sp][x] = (T)0;
+          }
+        }
+      }
+      if (SEG) {
+        // runs of consecutive lanes whose kets share shell c (first AO
+        // ket.ao_a); inactive lanes form runs of their own
+        const int key = active ? ket.ao_a : -1 - lane;
+        const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+        const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || key != prev);
+        const unsigned later = heads & (0xfffffffeu << lane);
+        const int end = later ? __ffs(later) - 1 : 32;
+        const bool head = (heads >> lane) & 1u;
+        const int n = a.n, i0 = bra.ao_a, j0 = bra.ao_b, k0 = ket.ao_a;
+#pragma unroll
+        for (int sp = 0; sp < NS; ++sp) {
+          double* K = a.Kacc + (size_t)sp * n * n;
+#pragma unroll
+          for (int i = 0; i < NA; ++i)
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+              const T v = run_sum(kac[sp][i * NC + k], lane, end);
+              if (head && active) atomicAdd(K + (size_t)(i0 + i) * n + k0 + k, 2.0 * (double)v);
+            }
+#pragma unroll
+          for (int j = 0; j < NB; ++j)
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+              const T v = run_sum(kbc[sp][j * NC + k], lane, end);
+              if (head && active) atomicAdd(K + (size_t)(j0 + j) * n + k0 + k, 2.0 * (double)v);
+            }
+        }
       }
       // J'[a,b]: the whole warp shares the bra pair
 #pragma unroll

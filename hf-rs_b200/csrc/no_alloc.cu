@@ -138,7 +138,7 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
     a.nchunks = L.nchunks;
     a.nentries = (int)L.prefix[0];
     a.nwarps = L.prefix[1];
-    rc = hfg::cuda_check(ctx, hfg::launch_jk(L.la, L.lb, L.lc, L.ld, L.G, L.fp32, a, ctx->stream), "J/K launch");
+    rc = hfg::cuda_check(ctx, hfg::launch_jk(L.la, L.lb, L.lc, L.ld, L.fp32, a, ctx->stream), "J/K launch");
     if (rc != HFG_OK) return rc;
   }
   const int blk = 256;

@@ -12,7 +12,7 @@
 namespace hfg {
 
 __global__ void count_kernel(const JKEntry* __restrict__ entries, const long long* __restrict__ prefix, int nentries,
-                             long long nwarps, int G, const PairInfo* __restrict__ pairs,
+                             long long nwarps, const PairInfo* __restrict__ pairs,
                              const double* __restrict__ pairQ, double thr, const float* __restrict__ pbound,
                              double eps, unsigned long long* __restrict__ out) {
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -24,10 +24,9 @@ __global__ void count_kernel(const JKEntry* __restrict__ entries, const long lon
     if (prefix[mid] <= warp) lo = mid; else hi = mid;
   }
   const JKEntry e = entries[lo];
-  const int qpw = 32 / G, grp = lane / G, gl = lane - grp * G;
-  const int k = e.k_lo + (int)(warp - prefix[lo]) * qpw + grp;
+  const int k = e.k_lo + (int)(warp - prefix[lo]) * 32 + lane;
   unsigned long long c = 0, quartets = 0;
-  if (gl == 0 && k < e.k_hi && pairQ[k] * pairQ[e.bra] > thr) {
+  if (k < e.k_hi && pairQ[k] * pairQ[e.bra] > thr) {
     quartets = 1;
     const PairInfo b = pairs[e.bra], q = pairs[k];
     // the kernels' loop: ket primitive pairs surviving against the largest bra
@@ -54,12 +53,12 @@ __global__ void count_kernel(const JKEntry* __restrict__ entries, const long lon
   if (lane == 0 && quartets) atomicAdd(out + 1, quartets);
 }
 
-cudaError_t launch_count(const JKEntry* entries, const long long* prefix, int nentries, long long nwarps, int G,
+cudaError_t launch_count(const JKEntry* entries, const long long* prefix, int nentries, long long nwarps,
                          const PairInfo* pairs, const double* pairQ, double thr, const float* pbound, double eps,
                          unsigned long long* out, cudaStream_t st) {
   const long long threads = nwarps * 32;
   if (threads == 0) return cudaSuccess;
-  count_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(entries, prefix, nentries, nwarps, G, pairs, pairQ,
+  count_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(entries, prefix, nentries, nwarps, pairs, pairQ,
                                                                    thr, pbound, eps, out);
   return cudaGetLastError();
 }

@@ -166,6 +166,10 @@ def load_library():
     L.hfg_df_three_center.argtypes = [VP, P(HfgBasis), DP, ctypes.c_size_t]
     L.hfg_df_jk.argtypes = [VP, DP, ctypes.c_int, DP, DP, ctypes.c_int]
     L.hfg_df_last_stats.argtypes = [VP, DP, DP, DP]
+    L.hfg_df_jk_shard.argtypes = [VP, DP, ctypes.c_int, DP, DP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.hfg_df_jk_device_shard.argtypes = [VP, VP, ctypes.c_int, VP, VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.hfg_df_transform.argtypes = [VP, DP, ctypes.c_int, DP, ctypes.c_size_t]
+    L.hfg_df_mp2.argtypes = [VP, DP, DP, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP]
     L.hfg_scf_df.argtypes = [VP, VP, ctypes.c_int, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     L.hfg_server_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, P(VP)]
     L.hfg_server_submit.argtypes = [VP, P(Job)]
@@ -467,6 +471,36 @@ class DFTensor:
         J, K = np.zeros((n, n)), np.zeros((n, n))
         self.ctx._check(self.lib.hfg_df_jk(self.h, _dp(C), C.shape[1], _dp(J), _dp(K), mma))
         return J, K
+
+    def transform(self, C):
+        """The factor in the MO basis C (n x m): rank x m (m + 1) / 2 packed
+        (hfg_df_transform, DfTensor::transform)."""
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        m = C.shape[1]
+        rank = self.sizes()[1]
+        out = np.zeros((rank, m * (m + 1) // 2))
+        self.ctx._check(self.lib.hfg_df_transform(self.h, _dp(C), m, _dp(out), out.size))
+        return out
+
+    def mp2_energy(self, C, eps, n_occ, n_frozen=0):
+        """RI-MP2 correlation energy (hfg_df_mp2, DfTensor::mp2_energy)."""
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        e = np.ascontiguousarray(eps, dtype=np.float64)
+        out = ctypes.c_double()
+        self.ctx._check(self.lib.hfg_df_mp2(self.h, _dp(C), _dp(e), C.shape[1], n_occ, n_frozen, ctypes.byref(out)))
+        return out.value
+
+    def jk_shard(self, C_occ, shard, nshards, mma=HFG_DF_FP64):
+        """Partial J, K over the shard's auxiliary functions (hfg_df_jk_shard)."""
+        n = self.ctx.n
+        C = np.ascontiguousarray(C_occ, dtype=np.float64)
+        J, K = np.zeros((n, n)), np.zeros((n, n))
+        self.ctx._check(self.lib.hfg_df_jk_shard(self.h, _dp(C), C.shape[1], _dp(J), _dp(K), mma, shard, nshards))
+        return J, K
+
+    def jk_device_shard(self, d_C, nocc, d_J, d_K, shard, nshards, mma=HFG_DF_FP64):
+        """Device form (integer pointers; C column-major n x nocc)."""
+        self.ctx._check(self.lib.hfg_df_jk_device_shard(self.h, d_C, nocc, d_J, d_K, mma, shard, nshards))
 
     def last_stats(self):
         """Device time (ms), executed tensor-core flops and non-zero tile share

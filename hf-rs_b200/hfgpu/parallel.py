@@ -37,3 +37,23 @@ class ShardedJK:
             dist.all_reduce(J, op=dist.ReduceOp.SUM, group=self.group)
             dist.all_reduce(K, op=dist.ReduceOp.SUM, group=self.group)
         return J, K
+
+
+def aux_shard_range(rank, shard, nshards):
+    """Auxiliary functions [lo, hi) of DF shard `shard` of `nshards` (the
+    split hfg_df_jk_device_shard uses)."""
+    return rank * shard // nshards, rank * (shard + 1) // nshards
+
+
+class ShardedDFJK(ShardedJK):
+    """DF J/K of occupied coefficients on all ranks: each rank sums over its
+    range of auxiliary functions (hfg_df_jk_device_shard) and one all-reduce
+    adds the partial J and K (hf-rs's map-reduce over Q, src/df.rs:143-173).
+    Call with (C, None, J, K): C column-major n x nocc (a torch tensor whose
+    storage is the n x nocc block of a column-major matrix), J and K n x n."""
+
+    def __init__(self, rank, world, df, nocc, mma=0, group=None):
+        def build(C, _unused, J, K, shard, nshards):
+            df.jk_device_shard(C.data_ptr(), nocc, J.data_ptr(), K.data_ptr(), shard, nshards, mma=mma)
+
+        super().__init__(rank, world, build=build, group=group)

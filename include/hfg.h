@@ -240,6 +240,38 @@ int hfg_df_three_center(hfg_ctx* ctx, const hfg_basis* aux, double* out, size_t 
  */
 int hfg_df_jk(hfg_df* df, const double* C_occ, int nocc, double* J, double* K, int mma);
 /*
+ * One shard of hfg_df_jk for a multi-GPU DF build (no hf-rs counterpart:
+ * hf-rs's loop over the auxiliary index Q is one Rayon map-reduce,
+ * src/df.rs:143-173).  Shard s of N sums J and K over the auxiliary functions
+ * [s R / N, (s + 1) R / N) of the factor's R; the shards' J and K add up to
+ * hfg_df_jk's (one all-reduce of 2 n^2 doubles).  Host buffers as hfg_df_jk.
+ */
+int hfg_df_jk_shard(hfg_df* df, const double* C_occ, int nocc, double* J, double* K, int mma, int shard,
+                    int nshards);
+/*
+ * As hfg_df_jk_shard with device pointers on the context stream: d_C is the
+ * occupied block column-major (n x nocc, leading dimension n), d_J and d_K
+ * are n x n.
+ */
+int hfg_df_jk_device_shard(hfg_df* df, const double* d_C, int nocc, double* d_J, double* d_K, int mma, int shard,
+                           int nshards);
+/*
+ * Stands in for DfTensor::transform (src/df.rs:182-210): the factor in the MO
+ * basis C (host, row-major n x m, hf-rs's Matrix with m MO columns),
+ * out[Q][compound_index(p, q)] = (C^T B_Q C)[p][q] for p >= q, row-major
+ * rank x m (m + 1) / 2 (len must equal that).  FP64 on the stored factor.
+ */
+int hfg_df_transform(hfg_df* df, const double* C, int m, double* out, size_t len);
+/*
+ * Stands in for DfTensor::transform(C) followed by mp2_energy(eps, n_occ,
+ * n_frozen) (src/df.rs:182-236): the closed-shell RI-MP2 correlation energy
+ * in the canonical MO basis C (row-major n x m) with orbital energies eps[m]
+ * and the n_frozen lowest occupied orbitals frozen.  Rejects an invalid
+ * partition (HFG_ERR_INVALID_INPUT) and a denominator within 1e-12 of zero
+ * (HFG_ERR_SCF, hf-rs's HfError::Response).
+ */
+int hfg_df_mp2(hfg_df* df, const double* C, const double* eps, int m, int n_occ, int n_frozen, double* energy);
+/*
  * No counterpart in hf-rs.  Device time (ms) of the exchange (K) of the last
  * tensor-core hfg_df_jk on this factor, the tensor-core flops it executed
  * (both GEMMs, zero tiles skipped, lower triangle of K only), and the share

@@ -115,3 +115,58 @@ def test_df_rhf_sad_start_reaches_the_same_energy():
     assert rc["converged"] and rs["converged"]
     assert abs(rc["energy"] - rs["energy"]) < 1e-9
     assert rs["iterations"] < rc["iterations"]
+
+
+@pytest.mark.parametrize("mma", [HFG_DF_FP64, HFG_DF_BF16])
+def test_df_shards_over_the_auxiliary_index_sum_to_the_full_build(mma):
+    # the multi-GPU DF decomposition run shard after shard on one GPU
+    atoms = water_cluster(2)
+    ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
+    aux = CartesianBasis.build(atoms, "def2-universal-jkfit")
+    d = DFTensor(ctx, aux, storage=HFG_DF_FP64 if mma == HFG_DF_FP64 else HFG_DF_FP32)
+    C = occ_coeffs(ctx.n, 10, 6)
+    J0, K0 = d.jk(C, mma=mma)
+    for nshards in (2, 3):
+        Js, Ks = np.zeros_like(J0), np.zeros_like(K0)
+        for s in range(nshards):
+            J, K = d.jk_shard(C, s, nshards, mma=mma)
+            Js += J
+            Ks += K
+        tol = 1e-11 if mma == HFG_DF_FP64 else 1e-5 * np.max(np.abs(K0))
+        assert np.max(np.abs(Js - J0)) < 1e-11 and np.max(np.abs(Ks - K0)) < tol, (mma, nshards)
+    ctx.close()
+
+
+def test_df_transform_matches_the_oracle_factor_in_the_mo_basis():
+    # DfTensor::transform (src/df.rs:182-210): C^T B_Q C packed over p >= q
+    ctx = Context(CartesianBasis.build(ATOMS, "sto-3g"))
+    aux = CartesianBasis.build(ATOMS, "def2-svp-ri")
+    r = ctx.scf(tol=1e-12, want=("C", "eps"))
+    C = r["C"][0]
+    Bmo = DFTensor(ctx, aux).transform(C)
+    B = O.df_tensor(O.build_basis(ATOMS, O.load_basis("sto-3g")), O.build_basis(ATOMS, O.load_basis("def2-svp-ri")))
+    n, m = C.shape
+    iu = np.tril_indices(m)
+    ref = np.stack([(C.T @ O.unpack_pairs(B[q:q + 1], n)[0] @ C)[iu] for q in range(B.shape[0])])
+    assert Bmo.shape == ref.shape
+    # the rows depend on the metric's eigenvector basis (signs, order,
+    # degenerate rotations); the fitted MO integrals (pq|rs) = B^T B do not
+    assert np.max(np.abs(Bmo.T @ Bmo - ref.T @ ref)) < 1e-10
+    ctx.close()
+
+
+def test_ri_mp2_matches_golden(golden_dir):
+    # hf-rs tests/df_test.rs:22-71: RHF (tol 1e-13), DF factor with metric
+    # cutoff 1e-10, RI-MP2 in the canonical MO basis within 1e-9 Eh of PySCF
+    g = np.load(os.path.join(golden_dir, "df.npz"))
+    ctx = Context(CartesianBasis.build(ATOMS, "sto-3g"))
+    r = ctx.scf(tol=1e-13, max_iter=150, want=("C", "eps"))
+    assert r["converged"]
+    df = DFTensor(ctx, CartesianBasis.build(ATOMS, "def2-svp-ri"))
+    e = df.mp2_energy(r["C"][0], r["eps"][0], n_occ=5)
+    assert abs(e - float(g["ri_mp2"])) < 1e-9, (e, float(g["ri_mp2"]))
+    # a frozen core changes the energy; an invalid partition is rejected
+    assert df.mp2_energy(r["C"][0], r["eps"][0], n_occ=5, n_frozen=1) > e
+    with pytest.raises(Exception):
+        df.mp2_energy(r["C"][0], r["eps"][0], n_occ=5, n_frozen=6)
+    ctx.close()
