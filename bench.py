@@ -581,16 +581,30 @@ def measure_df(args, torch):
             ts.append(time.time() - t0)
         return min(ts), r
 
+    # the reference: FP64 arithmetic on an FP64 factor; above (H2O)64 an FP64
+    # factor does not fit next to the FP32 one, and FP64 arithmetic on the
+    # FP32 factor stands in (its K differs from the FP64 factor's by the
+    # storage rounding only)
+    big = args.df_waters > 64
+    d32 = None
+    if not big:
+        t0 = time.time()
+        d64 = DFTensor(ctx, aux, pair_threshold=1e-12, storage=HFG_DF_FP64)
+        out["fp64"] = {"build_s": time.time() - t0, "factor": "FP64"}
     t0 = time.time()
-    d64 = DFTensor(ctx, aux, pair_threshold=1e-12, storage=HFG_DF_FP64)
-    out["fp64"] = {"build_s": time.time() - t0}
-    t64, (J64, K64) = wall(lambda: d64.jk(q, mma=HFG_DF_FP64), reps=2)
+    if big:
+        d32 = DFTensor(ctx, aux, pair_threshold=1e-12, storage=HFG_DF_FP32)
+        d64 = d32
+        out["fp64"] = {"factor": "FP32 (an FP64 factor does not fit at this size)"}
+    build32 = time.time() - t0
+    t64, (J64, K64) = wall(lambda: d64.jk(q, mma=HFG_DF_FP64), reps=1)
     naux, rank, ncol = d64.sizes()
     out["fp64"].update({"jk_s": t64, "rank": rank, "pairs": ncol, "arith": "FP64 (cuBLAS DGEMM)"})
-    d64.close()
-    t0 = time.time()
-    d32 = DFTensor(ctx, aux, pair_threshold=1e-12, storage=HFG_DF_FP32)
-    build32 = time.time() - t0
+    if not big:
+        d64.close()
+        t0 = time.time()
+        d32 = DFTensor(ctx, aux, pair_threshold=1e-12, storage=HFG_DF_FP32)
+        build32 = time.time() - t0
     alg = 4.0 * n * n * nocc * rank
     best = 0.0
     for name, mma, scale in (("tf32", HFG_DF_FP32, 0.5), ("bf16", HFG_DF_BF16, 1.0)):

@@ -679,8 +679,22 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
     for (auto& x : ev) cudaEventCreate(&x);
     cudaEventRecord(ev[0], ctx->stream);
   }
+  // The class launches are independent (each adds into J', K' with atomics):
+  // they are spread over the context stream and its side streams so that
+  // they run concurrently (parallel branches when captured into a graph).  A
+  // small molecule's build then costs about its slowest class instead of the
+  // sum over classes; a large one's persistent grids fill the GPU either way.
+  // Profiled builds stay on one stream (per-launch events).
+  const int nstreams = profile ? 1 : 1 + kJKSideStreams;
+  if (nstreams > 1) {
+    HFG_CUDA(ctx, ctx->ensure_side_streams());
+    HFG_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+    for (int k = 0; k < kJKSideStreams; ++k) HFG_CUDA(ctx, cudaStreamWaitEvent(ctx->side[k], ctx->ev_fork, 0));
+  }
   for (size_t l = 0; l < plan->launches.size(); ++l) {
     const Launch& L = plan->launches[l];
+    const int si = (int)(l % (size_t)nstreams);
+    cudaStream_t ls = si == 0 ? ctx->stream : ctx->side[si - 1];
     a.counter = ctx->d_counters.p + l;
     a.entries = L.d_entries;
     a.prefix = L.d_prefix;
@@ -704,8 +718,14 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
     a.nchunks = c1 - c0;
     a.nentries = (int)L.prefix[0];
     a.nwarps = L.prefix[1];
-    HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.fp32, a, ctx->stream));
+    HFG_CUDA(ctx, launch_jk(L.la, L.lb, L.lc, L.ld, L.fp32, a, ls));
     if (profile) cudaEventRecord(ev[l + 1], ctx->stream);
+  }
+  if (nstreams > 1) {
+    for (int k = 0; k < kJKSideStreams; ++k) {
+      HFG_CUDA(ctx, cudaEventRecord(ctx->ev_join[k], ctx->side[k]));
+      HFG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join[k], 0));
+    }
   }
   if (profile) {
     cudaEventSynchronize(ev.back());
@@ -794,6 +814,11 @@ hfg_ctx::~hfg_ctx() {
   d_J.release();
   d_K.release();
   d_tmp.release();
+  for (auto& x : side)
+    if (x) cudaStreamDestroy(x);
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  for (auto& x : ev_join)
+    if (x) cudaEventDestroy(x);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 

@@ -98,10 +98,31 @@ template <typename T> struct DevBuf {
 
 }  // namespace hfg
 
+namespace hfg {
+// side streams on which a J/K build's class launches run next to the
+// context stream
+constexpr int kJKSideStreams = 3;
+}  // namespace hfg
+
 struct hfg_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // fork / join of a J/K build's class launches (created on first use)
+  cudaStream_t side[hfg::kJKSideStreams] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[hfg::kJKSideStreams] = {};
+  cudaError_t ensure_side_streams() {
+    if (ev_fork) return cudaSuccess;
+    for (auto& x : side) {
+      const cudaError_t e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return e;
+    }
+    for (auto& x : ev_join) {
+      const cudaError_t e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming);
+  }
   std::mutex mu;
   std::string err;
 

@@ -821,11 +821,25 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
   std::vector<double> Bm;  // DIIS overlap matrix (count x count), host
   std::vector<int> slot;   // history slot of each stored vector, oldest first
   CK(cudaMemcpyAsync(Pprev.p, P.p, nspin * nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  // HFG_SCF_PROFILE=1: wall time of the iteration phases (the stream is
+  // synchronised at each phase boundary), printed on stderr
+  static const bool profile = getenv("HFG_SCF_PROFILE") && getenv("HFG_SCF_PROFILE")[0] == '1';
+  double ph_ms[4] = {0, 0, 0, 0};  // Fock build, convergence tests, DIIS, diagonalisation
+  auto ph_t = std::chrono::steady_clock::now();
+  auto phase = [&](int k) {
+    if (!profile) return;
+    cudaStreamSynchronize(ctx->stream);
+    const auto t = std::chrono::steady_clock::now();
+    ph_ms[k] += std::chrono::duration<double, std::milli>(t - ph_t).count();
+    ph_t = t;
+  };
   for (it = 1; it <= o->max_iter; ++it) {
+    phase(3);
     // incremental (mixed mode): the mixed phase, then the FP64 refinement
     // from one full FP64 build
     if (incremental) RK(fock_inc(refining ? jo64 : jo));
     else RK(fock(refining ? jo64 : jo));
+    phase(0);
     if (refining) ++refine_done;
     e_tot = energy() + e_nuc;
     const double de = std::fabs(e_tot - prev_e);
@@ -861,6 +875,7 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
       refining = true;
     }
     CK(cudaMemcpyAsync(Pprev.p, P.p, nspin * nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    phase(1);
     // CDIIS push (drop the oldest when full) and extrapolate
     int sl;
     if (count < hist) {
@@ -920,6 +935,7 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
         }
       }
     }
+    phase(2);
     for (int sp = 0; sp < nspin; ++sp) {
       double* Pn = uhf ? s.tmp2.p : P.p;
       RK(diag(Fuse[sp], C.p + sp * (long long)n * m, Pn, s.evals.p, nocc[sp]));
@@ -930,6 +946,10 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
       }
     }
   }
+  phase(3);
+  if (profile)
+    fprintf(stderr, "hfg-profile scf n %d m %d iterations %d: fock %.1f ms, convergence tests %.1f ms, DIIS %.1f ms, "
+                    "diagonalisation %.1f ms\n", n, m, it, ph_ms[0], ph_ms[1], ph_ms[2], ph_ms[3]);
   if (it > o->max_iter) it = o->max_iter;
   // final orbitals from the true Fock matrix (src/scf.rs:579-597)
   if (!converged) RK(fock(jo64));
