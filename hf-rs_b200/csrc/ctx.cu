@@ -1013,7 +1013,10 @@ int hfg_jk(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* Pt, c
 // Packed tensor on the device: every quartet of the FP64 plan without
 // primitive screening (the plan holds each unique significant shell quartet
 // once), stored by eri_packed_kernel.
-static int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len) {
+}  // extern "C"
+
+namespace hfg {
+int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len) {
   const size_t n = (size_t)ctx->n, np = n * (n + 1) / 2;
   if (len != np * (np + 1) / 2)
     return set_error(ctx, HFG_ERR_INVALID_INPUT, "packed length must be n_p (n_p + 1) / 2 with n_p = n (n + 1) / 2");
@@ -1029,6 +1032,9 @@ static int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len
   }
   return HFG_OK;
 }
+}  // namespace hfg
+
+extern "C" {
 
 int hfg_eri_packed_device(hfg_ctx* ctx, double schwarz_threshold, double* d_out, size_t len) {
   if (!ctx) return HFG_ERR_INVALID_INPUT;

@@ -333,6 +333,7 @@ int hfg_df_sizes(const hfg_df* df, int* naux, int* rank, long long* ncol) {
 
 int hfg_df_metric(hfg_df* df, double* M) {
   if (!df || !M) return HFG_ERR_INVALID_INPUT;
+  if (!df->metric.p) return set_error(df->ctx, HFG_ERR_INVALID_INPUT, "this factor has no fitting metric (Cholesky vectors)");
   cudaSetDevice(df->ctx->device);
   const size_t len = (size_t)df->naux * df->naux;
   if (cudaMemcpy(M, df->metric.p, len * 8, cudaMemcpyDeviceToHost) != cudaSuccess)

@@ -174,6 +174,9 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
 int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs,
                      double* dJ, double* dK, int shard = 0, int nshards = 1);
 int set_error(hfg_ctx* ctx, int code, const std::string& msg);
+// Implemented in ctx.cu: the packed 8-fold ERI tensor on the device (length
+// n_p (n_p + 1) / 2), quartets with Q_ab Q_cd > thr; the context lock held.
+int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len);
 int build_shell_list(hfg_ctx* ctx, const hfg_basis* b, int lmax);
 void make_pair(const hfg_ctx* ctx, int a, int b, PairInfo& pi, std::vector<PrimPair>& pp, int owner);
 int cuda_check(hfg_ctx* ctx, cudaError_t e, const char* what);

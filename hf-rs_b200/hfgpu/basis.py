@@ -14,9 +14,9 @@ import os
 import numpy as np
 
 DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "basis_data")
-SYMBOLS = ["H", "He", "Li", "Be", "B", "C", "N", "O", "F", "Ne"]
+SYMBOLS = ["H", "He", "Li", "Be", "B", "C", "N", "O", "F", "Ne", "Na", "Mg", "Al", "Si", "P", "S", "Cl", "Ar"]
 SHELL_L = {"S": 0, "P": 1, "D": 2, "F": 3, "G": 4, "H": 5, "I": 6, "K": 7}
-FILES = {"sto-3g": "sto-3g.gbs", "6-31g*": "6-31gstar.gbs", "cc-pvdz": "cc-pvdz.gbs",
+FILES = {"sto-3g": "sto-3g.gbs", "6-31g*": "6-31gstar.gbs", "6-31g": "6-31g.gbs", "cc-pvdz": "cc-pvdz.gbs",
          "def2-universal-jkfit": "def2-universal-jkfit.gbs", "def2-svp-ri": "def2-svp-ri.gbs"}
 
 

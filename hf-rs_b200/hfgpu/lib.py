@@ -170,6 +170,8 @@ def load_library():
     L.hfg_df_jk_device_shard.argtypes = [VP, VP, ctypes.c_int, VP, VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.hfg_df_transform.argtypes = [VP, DP, ctypes.c_int, DP, ctypes.c_size_t]
     L.hfg_df_mp2.argtypes = [VP, DP, DP, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP]
+    L.hfg_cholesky_eri.argtypes = [VP, ctypes.c_double, ctypes.c_size_t, P(VP), DP, P(ctypes.c_longlong), ctypes.c_int,
+                                   P(ctypes.c_int)]
     L.hfg_scf_df.argtypes = [VP, VP, ctypes.c_int, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     L.hfg_server_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, P(VP)]
     L.hfg_server_submit.argtypes = [VP, P(Job)]
@@ -508,6 +510,23 @@ class DFTensor:
         ms, fl, tf = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         self.ctx._check(self.lib.hfg_df_last_stats(self.h, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(tf)))
         return {"k_ms": ms.value, "k_flops": fl.value, "tiles_fraction": tf.value}
+
+    @classmethod
+    def cholesky(cls, ctx, threshold, budget=512 * 1024 * 1024):
+        """Pivoted Cholesky vectors of the AO ERIs as a factor
+        (hfg_cholesky_eri, pivoted_cholesky_eri); returns (factor, pivots,
+        largest residual diagonal)."""
+        self = cls.__new__(cls)
+        self.ctx, self.lib, self.aux = ctx, ctx.lib, None
+        h = VP()
+        npair = ctx.n * (ctx.n + 1) // 2
+        piv = (ctypes.c_longlong * npair)()
+        cnt, mres = ctypes.c_int(), ctypes.c_double()
+        ctx._check(self.lib.hfg_cholesky_eri(ctx.h, threshold, budget, ctypes.byref(h), ctypes.byref(mres), piv, npair,
+                                             ctypes.byref(cnt)))
+        self.h = h
+        ctx._adopt(self)
+        return self, [int(piv[k]) for k in range(cnt.value)], mres.value
 
     def close(self):
         # a context that is already gone took its DF tensors with it

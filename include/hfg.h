@@ -272,6 +272,20 @@ int hfg_df_transform(hfg_df* df, const double* C, int m, double* out, size_t len
  */
 int hfg_df_mp2(hfg_df* df, const double* C, const double* eps, int m, int n_occ, int n_frozen, double* energy);
 /*
+ * Stands in for pivoted_cholesky_eri (src/cholesky.rs:42-190): the pivoted
+ * Cholesky vectors of the AO ERI supermatrix, (pq|rs) ~ sum_K L_K(pq) L_K(rs),
+ * to a largest residual diagonal <= threshold, as a factor handle over every
+ * packed AO pair (hfg_df_jk and hfg_scf_df then run Cholesky-factorised RHF,
+ * run_cd_hf).  The pivot is the largest residual diagonal, ties within 1e-12
+ * relative going to the smallest packed index.  `budget` bounds the stored
+ * vectors' bytes (hf-rs's CD_HF_FACTOR_BUDGET is 512 MiB); the supermatrix
+ * itself is held on the device (n_p (n_p + 1) / 2 doubles, n_p = n (n + 1) / 2).
+ * Outputs the largest residual diagonal, the pivots in selection order (up
+ * to max_pivots of them) and their count.
+ */
+int hfg_cholesky_eri(hfg_ctx* ctx, double threshold, size_t budget, hfg_df** out, double* max_residual,
+                     long long* pivots, int max_pivots, int* n_pivots);
+/*
  * No counterpart in hf-rs.  Device time (ms) of the exchange (K) of the last
  * tensor-core hfg_df_jk on this factor, the tensor-core flops it executed
  * (both GEMMs, zero tiles skipped, lower triangle of K only), and the share

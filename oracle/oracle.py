@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 BASIS_DIR = os.path.join(os.path.dirname(HERE), "hf-rs_b200", "hfgpu", "basis_data")
 ANG_TO_BOHR = 1.8897261246257702  # src/basis.rs:39
 
-SYMBOLS = ["H", "He", "Li", "Be", "B", "C", "N", "O", "F", "Ne"]
+SYMBOLS = ["H", "He", "Li", "Be", "B", "C", "N", "O", "F", "Ne", "Na", "Mg", "Al", "Si", "P", "S", "Cl", "Ar"]
 
 
 def build_library():
@@ -162,7 +162,7 @@ def parse_gaussian94(text):
 
 
 def load_basis(name):
-    fn = {"sto-3g": "sto-3g.gbs", "6-31g*": "6-31gstar.gbs", "cc-pvdz": "cc-pvdz.gbs",
+    fn = {"sto-3g": "sto-3g.gbs", "6-31g*": "6-31gstar.gbs", "6-31g": "6-31g.gbs", "cc-pvdz": "cc-pvdz.gbs",
           "def2-universal-jkfit": "def2-universal-jkfit.gbs", "def2-svp-ri": "def2-svp-ri.gbs"}[name.lower()]
     with open(os.path.join(BASIS_DIR, fn)) as f:
         return parse_gaussian94(f.read())
@@ -792,8 +792,104 @@ def df_rhf(atoms, basis, aux, charge=0, max_iter=100, e_tol=1e-12, r_tol=1e-10, 
            spherical=False):
     """src/hf_variants/ri_df_hf.rs:122-263 (run_df_hf_with_aux ->
     run_factorized_rhf)."""
+    return factorized_rhf(atoms, basis, df_tensor(basis, aux, cutoff), charge, max_iter, e_tol, r_tol, d_tol,
+                          spherical)
+
+
+def pivoted_cholesky(basis, threshold, budget=512 * 1024 * 1024):
+    """src/cholesky.rs:42-190: pivoted Cholesky vectors L (rank x n_pair, packed
+    compound_index columns) of the ERI supermatrix, the pivots and the
+    largest residual diagonal.  Columns of a pivot's shell pair come from
+    complete shell quartets with Q_ab Q_cd > 1e-15; the largest residual
+    diagonal is the pivot, ties within 1e-12 (relative) going to the smallest
+    packed index."""
     n = len(basis)
-    B = df_tensor(basis, aux, cutoff)
+    shells = shell_ranges(basis)
+    ns = len(shells)
+    npair = n * (n + 1) // 2
+    shell_of = np.zeros(n, dtype=int)
+    for s, (st, ct) in enumerate(shells):
+        shell_of[st:st + ct] = s
+    sl = [basis[st:st + ct] for st, ct in shells]
+    sp_index = lambda a, b: a * (a + 1) // 2 + b
+    diag = np.zeros(npair)
+    for a in range(ns):
+        for b in range(a + 1):
+            blk = shell_quartet(sl[a], sl[b], sl[a], sl[b])
+            na, nb = shells[a][1], shells[b][1]
+            for i in range(na):
+                for j in range(nb):
+                    p, q = shells[a][0] + i, shells[b][0] + j
+                    if p < q:
+                        continue
+                    ij = i * nb + j
+                    diag[p * (p + 1) // 2 + q] = blk[ij * na * nb + ij]
+    scale = max(float(diag.max()), 1.0)
+    if np.any(diag < -1e-12 * scale):
+        raise ValueError("negative ERI diagonal")
+    schw = np.zeros(ns * (ns + 1) // 2)
+    for p in range(n):
+        for q in range(p + 1):
+            k = sp_index(shell_of[p], shell_of[q])
+            schw[k] = max(schw[k], math.sqrt(max(diag[p * (p + 1) // 2 + q], 0.0)))
+    pairs = [(a, b) for a in range(ns) for b in range(a + 1)]
+
+    def columns(spi):
+        r, s_ = pairs[spi]
+        cols = {}
+        for pq, (a, b) in enumerate(pairs):
+            if not schw[pq] * schw[spi] > 1e-15:
+                continue
+            blk = shell_quartet(sl[a], sl[b], sl[r], sl[s_])
+            na, nb, nr, nss = shells[a][1], shells[b][1], shells[r][1], shells[s_][1]
+            for k in range(nr):
+                for l in range(nss):
+                    rr, ss = shells[r][0] + k, shells[s_][0] + l
+                    if rr < ss:
+                        continue
+                    col = cols.setdefault(rr * (rr + 1) // 2 + ss, np.zeros(npair))
+                    for i in range(na):
+                        for j in range(nb):
+                            p, q = shells[a][0] + i, shells[b][0] + j
+                            if p >= q:
+                                col[p * (p + 1) // 2 + q] = blk[((i * nb + j) * nr + k) * nss + l]
+        return cols
+
+    factors, pivots, cache = [], [], (None, None)
+    while True:
+        largest = float(diag.max())
+        pivot = int(np.nonzero(diag >= largest - 1e-12 * abs(largest))[0][0])
+        maximum = float(diag[pivot])
+        if maximum <= threshold or len(factors) == npair:
+            max_res = max(maximum, 0.0)
+            break
+        if 8 * npair * (len(factors) + 2) > budget:
+            raise ValueError("factor storage exceeds the memory budget")
+        p = int((math.isqrt(8 * pivot + 1) - 1) // 2)
+        q = pivot - p * (p + 1) // 2
+        spi = sp_index(max(shell_of[p], shell_of[q]), min(shell_of[p], shell_of[q]))
+        if cache[0] != spi:
+            cache = (spi, columns(spi))
+        col = cache[1].get(pivot, np.zeros(npair))
+        root = math.sqrt(maximum)
+        L = np.array(factors) if factors else np.zeros((0, npair))
+        row = (col - (L[:, pivot] @ L if len(factors) else 0.0)) / root
+        row[pivot] = root
+        diag = diag - row * row
+        if np.any(diag < -1e-10 * scale):
+            raise ValueError("nonpositive residual Coulomb diagonal")
+        diag = np.maximum(diag, 0.0)
+        factors.append(row)
+        pivots.append(pivot)
+    if not factors:
+        raise ValueError("threshold exceeds every ERI diagonal")
+    return np.array(factors), pivots, max_res
+
+
+def factorized_rhf(atoms, basis, B, charge=0, max_iter=100, e_tol=1e-12, r_tol=1e-10, d_tol=1e-10, spherical=False):
+    """src/hf_variants/ri_df_hf.rs:160-263 (run_factorized_rhf) on a given
+    factor B (DF or Cholesky vectors)."""
+    n = len(basis)
     nel = sum(SYMBOLS.index(s.capitalize()) + 1 for s, _ in atoms) - charge
     no = nel // 2
     S, T, V = one_electron(basis, atoms)

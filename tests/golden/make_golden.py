@@ -12,6 +12,9 @@ reference tree:
                      Cartesian ERIs with their (i,j,k,l) indices
   scf_energies.json  scf_reference.json: RHF/UHF energies (STO-3G, 6-31G*)
   water_ccpvdz.json  spherical_reference.json["systems"]["water_ccpvdz"]
+  cd_hf.json         cd_hf_reference.json: pivoted-Cholesky pivots, vector
+                     counts, residuals and CD-HF energies (LiH STO-3G,
+                     water and HCl 6-31G)
   df.npz             df_reference.json: metric, (P|mn) and the RI-MP2 energy
                      for water STO-3G / def2-SVP-RI, and the
                      df_hf_reference.json "water" case
@@ -68,6 +71,15 @@ def main(root):
                         three=np.array(df["three"]), water_atoms=np.array(json.dumps(c["atoms"])),
                         e_scf=c["e_scf"], P=np.array(c["density"]), F=np.array(c["fock"]),
                         J=np.array(c["j"]), K=np.array(c["k"]), n_aux=c["n_aux"], ri_mp2=df["ri_mp2"])
+    cd = json.load(open(os.path.join(data, "cd_hf_reference.json")))
+    cases = []
+    for c in cd["cases"]:
+        cases.append({"name": c["name"], "basis": {"STO_3G_GBS": "sto-3g", "BASIS_6_31G_GBS": "6-31g"}[c["basis_constant"]],
+                      "atoms": [[a["symbol"], a["position"]] for a in c["atoms"]], "e_rhf": c["e_rhf"],
+                      "thresholds": [{k: t[k] for k in ("threshold", "n_vectors", "pivots", "max_residual", "e_cd_hf")}
+                                     for t in c["thresholds"]]})
+    json.dump({"source": "hf-rs tests/data/cd_hf_reference.json (" + cd["source"] + ")", "cases": cases},
+              open(os.path.join(HERE, "cd_hf.json"), "w"), indent=1)
     print("fixtures written to", HERE)
 
 

@@ -189,3 +189,22 @@ def test_df_metric_three_centre_and_dfhf(golden_dir):
     assert abs(r["energy"] - float(g["e_scf"])) < 1e-9
     for k in ("P", "F", "J", "K"):
         assert np.max(np.abs(r[k] - g[k])) < 1e-9, k
+
+
+def test_pivoted_cholesky_and_cd_hf_match_golden(golden_dir):
+    # hf-rs tests/cd_hf_test.rs:42-70: pivot sequence, vector count and
+    # largest residual (1e-12) of the pivoted Cholesky ERI factor, and the
+    # CD-HF energy (run_cd_hf, tol 1e-12) within 1e-9 Eh
+    d = json.load(open(os.path.join(golden_dir, "cd_hf.json")))
+    for c in d["cases"]:
+        atoms = [(a[0], tuple(a[1])) for a in c["atoms"]]
+        basis = O.build_basis(atoms, O.load_basis(c["basis"]))
+        for t in c["thresholds"]:
+            L, piv, mres = O.pivoted_cholesky(basis, t["threshold"])
+            assert L.shape[0] == t["n_vectors"], (c["name"], t["threshold"])
+            assert piv == t["pivots"], (c["name"], t["threshold"])
+            assert mres <= t["threshold"] and abs(mres - t["max_residual"]) < 1e-12
+            tol = 1e-12
+            r = O.factorized_rhf(atoms, basis, L, max_iter=300, e_tol=tol, r_tol=max(tol ** 0.5 * 1e-2, 1e-11),
+                                 d_tol=min(max(tol ** 0.5 * 0.1, 1e-12), 1e-10))
+            assert abs(r["energy"] - t["e_cd_hf"]) < 1e-9, (c["name"], t["threshold"], r["energy"], t["e_cd_hf"])
