@@ -494,20 +494,24 @@ def measure_serving(args):
     """Served SCF stream vs sequential plain solves on a bounded sample of the
     seeded job stream (first `serve_jobs` jobs, waters uniform in
     {1..serve_max_waters}, bases uniform over STO-3G / 6-31G* / cc-pVDZ, 10%
-    UHF doublets).  Sequential: one FP64 solve at a time.  Served: 8 slots,
-    mixed precision with FP64 refinement, all jobs submitted at once (an
-    arrival rate above capacity); jobs under 256 basis functions run FP64."""
+    UHF doublets).  Sequential: one FP64 solve at a time, each with its own
+    builds.  Served: 8 slots, mixed precision with FP64 refinement, all jobs
+    submitted at once (an arrival rate above capacity); jobs under 256 basis
+    functions run FP64, and their RHF Fock builds are batched across the
+    running jobs."""
     from hfgpu.serve import MIXED, build_inputs, make_stream, run_stream, summarize
     jobs = make_stream(args.serve_jobs, rate=1000.0, max_waters=args.serve_max_waters, seed=4242)
     inputs = build_inputs(jobs)
-    seq, span_seq = run_stream(jobs, slots=1, budget_bytes=120 << 30, honour_arrivals=False, inputs=inputs)
+    seq, span_seq = run_stream(jobs, slots=1, budget_bytes=120 << 30, honour_arrivals=False, inputs=inputs,
+                               batch_max_ao=0)
+    batch = {}
     srv, span_srv = run_stream(jobs, slots=8, budget_bytes=120 << 30, honour_arrivals=False, inputs=inputs,
-                               jk=MIXED, mixed_min_ao=256)
+                               jk=MIXED, mixed_min_ao=256, batch_max_ao=256, stats_out=batch)
     a, b = summarize(seq, span_seq), summarize(srv, span_srv)
     de = max(abs(x["energy"] - y["energy"]) for x, y in zip(seq, srv) if x["status"] == 0 and y["status"] == 0)
     return {"sample": "%d jobs, waters 1..%d, STO-3G/6-31G*/cc-pVDZ, 10%% UHF" % (len(jobs), args.serve_max_waters),
             "sequential_fp64": a, "served_mixed_8_slots": b, "jobs_per_s_ratio": b["jobs_per_s"] / a["jobs_per_s"],
-            "max_abs_dE_served_vs_sequential": de}
+            "batched_fock_builds": batch, "max_abs_dE_served_vs_sequential": de}
 
 
 def measure_scf(waters, ctx, opt_mixed):

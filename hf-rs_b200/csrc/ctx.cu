@@ -583,6 +583,28 @@ __global__ void symmetrize_kernel(const double* __restrict__ acc, double* __rest
   out[t] = 0.5 * (acc[m * nn + (long long)i * n + j] + acc[m * nn + (long long)j * n + i]);
 }
 
+// One matrix of a batched build: its accumulator and (symmetrised) output.
+struct BatchMat {
+  double* acc;
+  double* out;
+  int n;
+};
+
+// Over the matrices of a batched build (blockIdx.y): zero the accumulators
+// (sym = 0) or write out = (acc + acc^T) / 2 (sym = 1).
+__global__ void batch_mats_kernel(const BatchMat* __restrict__ mats, int sym) {
+  const BatchMat m = mats[blockIdx.y];
+  const long long nn = (long long)m.n * m.n;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn; t += (long long)gridDim.x * blockDim.x) {
+    if (!sym) {
+      m.acc[t] = 0.0;
+    } else {
+      const long long i = t / m.n, j = t % m.n;
+      m.out[t] = 0.5 * (m.acc[t] + m.acc[j * m.n + i]);
+    }
+  }
+}
+
 // a -= b
 __global__ void axpy_sub_kernel(double* __restrict__ a, const double* __restrict__ b, long long len) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -623,6 +645,9 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   if (!(o.schwarz_threshold >= 0.0) || !(o.prim_threshold >= 0.0) ||
       (o.precision != HFG_FP64 && o.precision != HFG_MIXED))
     return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid J/K options");
+  // a context served with others hands its RHF builds to their batcher
+  if (ctx->batcher && nspin == 1 && nshards == 1 && dPs == dPt)
+    return batcher_submit(ctx->batcher, ctx, o, dPt, dJ, dK);
   Plan* plan = nullptr;
   int rc = build_plan(ctx, o.schwarz_threshold, o.mixed_threshold, o.prim_threshold, o.precision, plan);
   if (rc != HFG_OK) return rc;
@@ -1009,6 +1034,222 @@ int hfg_jk(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* Pt, c
   HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return HFG_OK;
 }
+
+int hfg_jk_device_batch(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, const double* const* d_P,
+                        double* const* d_J, double* const* d_K, void* stream) {
+  if (!ctxs || n_jobs < 1 || !ctxs[0]) return HFG_ERR_INVALID_INPUT;
+  hfg_ctx* c0 = ctxs[0];
+  if (!d_P || !d_J || !d_K) return set_error(c0, HFG_ERR_INVALID_INPUT, "null pointer");
+  for (int j = 0; j < n_jobs; ++j)
+    if (!ctxs[j]) return set_error(c0, HFG_ERR_INVALID_INPUT, "null pointer");
+  // each context's accumulators serve one molecule: no context twice
+  std::vector<hfg_ctx*> order(ctxs, ctxs + n_jobs);
+  std::sort(order.begin(), order.end());
+  if (std::adjacent_find(order.begin(), order.end()) != order.end())
+    return set_error(c0, HFG_ERR_INVALID_INPUT, "a context appears twice in the batch");
+  hfg_jk_opts o;
+  if (opts) o = *opts; else hfg_jk_opts_default(&o);
+  std::vector<hfg_jk_opts> per(n_jobs, o);
+  // lock in address order, so that concurrent batches cannot deadlock
+  std::vector<std::unique_lock<std::mutex>> locks;
+  locks.reserve(order.size());
+  for (hfg_ctx* c : order) locks.emplace_back(c->mu);
+  cudaSetDevice(c0->device);
+  return jk_batch_locked(ctxs, n_jobs, per.data(), d_P, d_J, d_K, stream ? (cudaStream_t)stream : c0->stream,
+                         nullptr);
+}
+
+}  // extern "C"
+
+namespace hfg {
+
+int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, const double* const* d_P,
+                    double* const* d_J, double* const* d_K, cudaStream_t st, BatchStaging* staging) {
+  hfg_ctx* c0 = ctxs[0];
+  // an error of the batch is reported on every context of it
+  auto fail = [&](int rc, const std::string& msg) {
+    for (int j = 0; j < n_jobs; ++j) set_error(ctxs[j], rc, msg);
+    return rc;
+  };
+  auto cuda = [&](cudaError_t e, const char* what) {
+    return e == cudaSuccess ? HFG_OK : fail(HFG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+#define BK(call)                                  \
+  do {                                            \
+    const int _rc = cuda((call), #call);          \
+    if (_rc != HFG_OK) return _rc;                \
+  } while (0)
+  if (n_jobs < 1 || n_jobs > 32767) return fail(HFG_ERR_INVALID_INPUT, "a batch holds 1 to 32767 molecules");
+  for (int j = 0; j < n_jobs; ++j) {
+    const hfg_jk_opts& o = opts[j];
+    if (!d_P[j] || !d_J[j] || !d_K[j]) return fail(HFG_ERR_INVALID_INPUT, "null pointer");
+    if (ctxs[j]->device != c0->device) return fail(HFG_ERR_INVALID_INPUT, "the contexts of a batch must share one device");
+    if (!(o.schwarz_threshold >= 0.0) || !(o.prim_threshold >= 0.0) ||
+        (o.precision != HFG_FP64 && o.precision != HFG_MIXED))
+      return fail(HFG_ERR_INVALID_INPUT, "invalid J/K options");
+  }
+  // per molecule: its plan (built once, cached on its context) and its
+  // accumulators, allocated on its own stream; then the batch stream waits
+  // for each context stream
+  std::vector<Plan*> plans(n_jobs, nullptr);
+  for (int j = 0; j < n_jobs; ++j) {
+    hfg_ctx* c = ctxs[j];
+    AllocScope alloc_scope(c->stream);
+    const hfg_jk_opts& o = opts[j];
+    const int rc = build_plan(c, o.schwarz_threshold, o.mixed_threshold, o.prim_threshold, o.precision, plans[j]);
+    if (rc != HFG_OK) return fail(rc, c->err);
+    const size_t nn = (size_t)c->n * c->n;
+    BK(c->d_Jacc.alloc(nn));
+    BK(c->d_Kacc.alloc(2 * nn));
+    BK(c->ensure_side_streams());
+    if (c->stream != st) {
+      BK(cudaEventRecord(c->ev_fork, c->stream));
+      BK(cudaStreamWaitEvent(st, c->ev_fork, 0));
+    }
+  }
+  // launch groups: the molecules' launches of one class and precision
+  struct Member {
+    int job;
+    const Launch* L;
+  };
+  using GroupKey = std::tuple<int, int, int, int, int>;
+  std::map<GroupKey, std::vector<Member>> groups;
+  for (int j = 0; j < n_jobs; ++j)
+    for (const Launch& L : plans[j]->launches)
+      if (L.nchunks > 0) groups[std::make_tuple(L.la, L.lb, L.lc, L.ld, (int)L.fp32)].push_back({j, &L});
+  std::vector<std::pair<GroupKey, const std::vector<Member>*>> glist;
+  for (const auto& kv : groups) glist.push_back({kv.first, &kv.second});
+  // most expensive classes first
+  std::stable_sort(glist.begin(), glist.end(), [](const auto& x, const auto& y) {
+    const auto& [a0, a1, a2, a3, a4] = x.first;
+    const auto& [b0, b1, b2, b3, b4] = y.first;
+    return std::make_tuple(a0 + a1 + a2 + a3, a4) > std::make_tuple(b0 + b1 + b2 + b3, b4);
+  });
+  // one device table for the call: counters, matrices, then per group its
+  // molecule table and first steps
+  const int ng = (int)glist.size();
+  auto align = [](size_t x) { return (x + 15) & ~(size_t)15; };
+  const size_t counters_bytes = sizeof(unsigned long long) * std::max(ng, 1);
+  size_t off = align(counters_bytes);
+  const size_t mats_off = off;
+  off = align(off + sizeof(BatchMat) * 2 * n_jobs);
+  std::vector<size_t> jobs_off(ng), steps_off(ng);
+  std::vector<long long> total(ng, 0);
+  for (int g = 0; g < ng; ++g) {
+    jobs_off[g] = off;
+    off = align(off + sizeof(JKJob) * glist[g].second->size());
+    steps_off[g] = off;
+    off = align(off + sizeof(long long) * glist[g].second->size());
+  }
+  // the tables go to pinned staging when they fit (an asynchronous copy),
+  // else through pageable memory
+  std::vector<unsigned char> pageable;
+  unsigned char* blob = nullptr;
+  if (staging && staging->host && off <= staging->bytes) {
+    BK(cudaEventSynchronize(staging->ev));
+    blob = static_cast<unsigned char*>(staging->host);
+  } else {
+    pageable.resize(off);
+    blob = pageable.data();
+  }
+  std::memset(blob, 0, off);
+  int maxn = 0;
+  {
+    BatchMat* mats = reinterpret_cast<BatchMat*>(blob + mats_off);
+    for (int j = 0; j < n_jobs; ++j) {
+      mats[2 * j] = {ctxs[j]->d_Jacc.p, d_J[j], ctxs[j]->n};
+      mats[2 * j + 1] = {ctxs[j]->d_Kacc.p, d_K[j], ctxs[j]->n};
+      maxn = std::max(maxn, ctxs[j]->n);
+    }
+  }
+  for (int g = 0; g < ng; ++g) {
+    JKJob* jt = reinterpret_cast<JKJob*>(blob + jobs_off[g]);
+    long long* stp = reinterpret_cast<long long*>(blob + steps_off[g]);
+    const auto& mem = *glist[g].second;
+    for (size_t k = 0; k < mem.size(); ++k) {
+      const int j = mem[k].job;
+      const hfg_ctx* c = ctxs[j];
+      const Launch& L = *mem[k].L;
+      JKJob& x = jt[k];
+      x.entries = L.d_entries;
+      x.prefix = L.d_prefix;
+      x.chunk_start = L.d_cstart;
+      x.chunk_entry = L.d_chunk;
+      x.pairs = c->d_pairs.p;
+      x.pairQ = c->d_pairQ.p;
+      x.rec64 = c->d_rec64.p;
+      x.rec32 = c->d_rec32.p;
+      x.pbound = c->d_pbound.p;
+      x.Dtot = d_P[j];
+      x.Jacc = c->d_Jacc.p;
+      x.Kacc = c->d_Kacc.p;
+      x.thr = opts[j].schwarz_threshold;
+      x.prim_eps = opts[j].prim_threshold;
+      x.n = c->n;
+      stp[k] = total[g];
+      total[g] += L.nchunks;
+    }
+  }
+  unsigned char* dev = nullptr;
+  BK(cudaMallocAsync((void**)&dev, off, st));
+  // released (stream-ordered, after the launches) on every return path
+  struct FreeAfter {
+    void* p;
+    cudaStream_t s;
+    ~FreeAfter() { cudaFreeAsync(p, s); }
+  } free_after{dev, st};
+  BK(cudaMemcpyAsync(dev, blob, off, cudaMemcpyHostToDevice, st));
+  if (blob != pageable.data()) BK(cudaEventRecord(staging->ev, st));
+  const BatchMat* d_mats = reinterpret_cast<const BatchMat*>(dev + mats_off);
+  const long long nnmax = (long long)maxn * maxn;
+  const dim3 mgrid((unsigned)std::min<long long>((nnmax + 255) / 256, 64), (unsigned)(2 * n_jobs));
+  batch_mats_kernel<<<mgrid, 256, 0, st>>>(d_mats, 0);
+  BK(cudaGetLastError());
+  // the groups run concurrently over the first context's side streams
+  BK(cudaEventRecord(c0->ev_fork, st));
+  for (int k = 0; k < kJKSideStreams; ++k) BK(cudaStreamWaitEvent(c0->side[k], c0->ev_fork, 0));
+  const int nstreams = 1 + kJKSideStreams;
+  for (int g = 0; g < ng; ++g) {
+    const auto& [la, lb, lc, ld, f32] = glist[g].first;
+    JKLaunchArgs a{};
+    a.boys64 = c0->d_boys64.p;
+    a.boys32 = c0->d_boys32.p;
+    a.expt64 = c0->d_expt64.p;
+    a.expt32 = c0->d_expt32.p;
+    a.nspin = 1;
+    a.counter = reinterpret_cast<unsigned long long*>(dev) + g;
+    a.jobs = reinterpret_cast<const JKJob*>(dev + jobs_off[g]);
+    a.job_steps = reinterpret_cast<const long long*>(dev + steps_off[g]);
+    a.njobs = (int)glist[g].second->size();
+    a.nchunks = total[g];
+    const int si = g % nstreams;
+    BK(launch_jk_batch(la, lb, lc, ld, f32 != 0, a, si == 0 ? st : c0->side[si - 1]));
+  }
+  for (int k = 0; k < kJKSideStreams; ++k) {
+    BK(cudaEventRecord(c0->ev_join[k], c0->side[k]));
+    BK(cudaStreamWaitEvent(st, c0->ev_join[k], 0));
+  }
+  batch_mats_kernel<<<mgrid, 256, 0, st>>>(d_mats, 1);
+  BK(cudaGetLastError());
+  // each context's later work (and reuse of its accumulators) follows the batch
+  cudaEvent_t done = nullptr;
+  BK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(done, st);
+  for (int j = 0; j < n_jobs && e == cudaSuccess; ++j)
+    if (ctxs[j]->stream != st) e = cudaStreamWaitEvent(ctxs[j]->stream, done, 0);
+  cudaEventDestroy(done);
+  BK(e);
+  for (int j = 0; j < n_jobs; ++j) {
+    ctxs[j]->last = plans[j]->stats;
+    ctxs[j]->last_plan = plans[j];
+  }
+#undef BK
+  return HFG_OK;
+}
+
+}  // namespace hfg
+
+extern "C" {
 
 // Packed tensor on the device: every quartet of the FP64 plan without
 // primitive screening (the plan holds each unique significant shell quartet

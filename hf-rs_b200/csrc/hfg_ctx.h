@@ -102,6 +102,9 @@ namespace hfg {
 // side streams on which a J/K build's class launches run next to the
 // context stream
 constexpr int kJKSideStreams = 3;
+// Collects the RHF J/K builds of several contexts into batched builds
+// (server.cu); a context with one set routes its builds through it.
+struct JKBatcher;
 }  // namespace hfg
 
 struct hfg_ctx {
@@ -110,11 +113,15 @@ struct hfg_ctx {
   bool own_stream = false;
   // fork / join of a J/K build's class launches (created on first use)
   cudaStream_t side[hfg::kJKSideStreams] = {};
+  hfg::JKBatcher* batcher = nullptr;  // RHF builds go through this batcher when set
   cudaEvent_t ev_fork = nullptr, ev_join[hfg::kJKSideStreams] = {};
   cudaError_t ensure_side_streams() {
     if (ev_fork) return cudaSuccess;
+    // the side streams take the context stream's priority
+    int prio = 0;
+    if (stream && cudaStreamGetPriority(stream, &prio) != cudaSuccess) prio = 0;
     for (auto& x : side) {
-      const cudaError_t e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
+      const cudaError_t e = cudaStreamCreateWithPriority(&x, cudaStreamNonBlocking, prio);
       if (e != cudaSuccess) return e;
     }
     for (auto& x : ev_join) {
@@ -174,6 +181,21 @@ int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK,
 int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt, const double* dPs,
                      double* dJ, double* dK, int shard = 0, int nshards = 1);
 int set_error(hfg_ctx* ctx, int code, const std::string& msg);
+// Pinned host memory for a batched build's tables, reused once `ev` (the
+// previous copy out of it) has completed.
+struct BatchStaging {
+  void* host = nullptr;
+  size_t bytes = 0;
+  cudaEvent_t ev = nullptr;
+};
+// Implemented in ctx.cu: RHF J/K of several contexts in one pass of batched
+// launches on `st` (molecule j with its own options opts[j]).  The caller
+// owns every context (their locks held, or their owners blocked).
+int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, const double* const* dP,
+                    double* const* dJ, double* const* dK, cudaStream_t st, BatchStaging* staging);
+// Implemented in server.cu: queue one RHF build with the batcher and wait
+// until the batch that takes it has been enqueued.
+int batcher_submit(JKBatcher* b, hfg_ctx* ctx, const hfg_jk_opts& o, const double* dP, double* dJ, double* dK);
 // Implemented in ctx.cu: the packed 8-fold ERI tensor on the device (length
 // n_p (n_p + 1) / 2), quartets with Q_ab Q_cd > thr; the context lock held.
 int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len);

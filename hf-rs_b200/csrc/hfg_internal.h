@@ -50,6 +50,25 @@ struct JKEntry {
   int bra, k_lo, k_hi, pad;
 };
 
+// One molecule of a batched J/K launch: its launch's work queue and the
+// buffers of its context (RHF: the total density is the spin density).
+struct JKJob {
+  const JKEntry* entries;
+  const long long* prefix;
+  const long long* chunk_start;
+  const int* chunk_entry;
+  const PairInfo* pairs;
+  const double* pairQ;
+  const PrimRec64* rec64;
+  const PrimRec32* rec32;
+  const float* pbound;
+  const double* Dtot;
+  double* Jacc;
+  double* Kacc;
+  double thr, prim_eps;  // the molecule's Schwarz and primitive thresholds
+  int n;
+};
+
 struct JKLaunchArgs {
   const JKEntry* entries;
   const long long* prefix;  // warp-task prefix over entries (size nentries + 1)
@@ -75,6 +94,10 @@ struct JKLaunchArgs {
   double* Kacc;        // nspin n x n
   int n, nspin;
   double prim_eps;
+  // batched launches: molecule table and the first step of each molecule
+  const JKJob* jobs;
+  const long long* job_steps;
+  int njobs;
 };
 
 }  // namespace hfg

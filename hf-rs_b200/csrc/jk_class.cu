@@ -14,13 +14,11 @@ namespace hfg {
 
 // Persistent grid: as many resident blocks as the kernel's occupancy allows
 // on every SM, capped by the work.
-template <typename T, int NS>
+template <typename T, int NS, bool BATCH = false>
 static cudaError_t launch_t(const JKLaunchArgs& a, cudaStream_t st) {
-  constexpr int L = EriClass<HFG_LA, HFG_LB, HFG_LC, HFG_LD>::L;
   constexpr int block = 256;
-  (void)L;
   const size_t smem = boys_smem_bytes<T>();
-  auto kern = jk_kernel<HFG_LA, HFG_LB, HFG_LC, HFG_LD, T, NS>;
+  auto kern = BATCH ? jk_batch_kernel<HFG_LA, HFG_LB, HFG_LC, HFG_LD, T> : jk_kernel<HFG_LA, HFG_LB, HFG_LC, HFG_LD, T, NS>;
   // resident blocks per device (a process may drive different device
   // models), looked up once per device
   constexpr int kMaxDev = 64;
@@ -45,6 +43,15 @@ static cudaError_t launch_t(const JKLaunchArgs& a, cudaStream_t st) {
 
 #define HFG_CAT2(a, b, c, d) launch_jk_##a##b##c##d
 #define HFG_CAT(a, b, c, d) HFG_CAT2(a, b, c, d)
+#define HFG_CATB2(a, b, c, d) launch_jkb_##a##b##c##d
+#define HFG_CATB(a, b, c, d) HFG_CATB2(a, b, c, d)
+
+// a batched launch over several molecules (RHF); a.nchunks is the total of
+// their steps
+cudaError_t HFG_CATB(HFG_LA, HFG_LB, HFG_LC, HFG_LD)(const JKLaunchArgs& a, bool fp32, cudaStream_t st) {
+  return fp32 ? launch_t<float, 1, true>(a, st) : launch_t<double, 1, true>(a, st);
+}
+
 cudaError_t HFG_CAT(HFG_LA, HFG_LB, HFG_LC, HFG_LD)(const JKLaunchArgs& a, bool fp32, cudaStream_t st) {
   if (a.nspin == 2) return fp32 ? launch_t<float, 2>(a, st) : launch_t<double, 2>(a, st);
   return fp32 ? launch_t<float, 1>(a, st) : launch_t<double, 1>(a, st);

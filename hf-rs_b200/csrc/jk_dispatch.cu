@@ -32,6 +32,34 @@ cudaError_t launch_jk(int la, int lb, int lc, int ld, bool fp32, const JKLaunchA
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_jk_batch(int la, int lb, int lc, int ld, bool fp32, const JKLaunchArgs& a, cudaStream_t st) {
+#define HFG_CASE(A, B, C, D) \
+  if (la == A && lb == B && lc == C && ld == D) return launch_jkb_##A##B##C##D(a, fp32, st);
+  HFG_CASE(0, 0, 0, 0)
+  HFG_CASE(1, 0, 0, 0)
+  HFG_CASE(1, 0, 1, 0)
+  HFG_CASE(1, 1, 0, 0)
+  HFG_CASE(1, 1, 1, 0)
+  HFG_CASE(1, 1, 1, 1)
+  HFG_CASE(2, 0, 0, 0)
+  HFG_CASE(2, 0, 1, 0)
+  HFG_CASE(2, 0, 1, 1)
+  HFG_CASE(2, 0, 2, 0)
+  HFG_CASE(2, 1, 0, 0)
+  HFG_CASE(2, 1, 1, 0)
+  HFG_CASE(2, 1, 1, 1)
+  HFG_CASE(2, 1, 2, 0)
+  HFG_CASE(2, 1, 2, 1)
+  HFG_CASE(2, 2, 0, 0)
+  HFG_CASE(2, 2, 1, 0)
+  HFG_CASE(2, 2, 1, 1)
+  HFG_CASE(2, 2, 2, 0)
+  HFG_CASE(2, 2, 2, 1)
+  HFG_CASE(2, 2, 2, 2)
+#undef HFG_CASE
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_schwarz(int la, int lb, const PairInfo* pairs, const PrimPair* prims, int first, int count,
                            const double* boys, const double* expt, double* out, int prim_mode, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;

@@ -6,7 +6,9 @@
 
 namespace hfg {
 
-#define HFG_DECL(a, b, c, d) cudaError_t launch_jk_##a##b##c##d(const JKLaunchArgs&, bool fp32, cudaStream_t);
+#define HFG_DECL(a, b, c, d)                                                            \
+  cudaError_t launch_jk_##a##b##c##d(const JKLaunchArgs&, bool fp32, cudaStream_t); \
+  cudaError_t launch_jkb_##a##b##c##d(const JKLaunchArgs&, bool fp32, cudaStream_t);
 HFG_DECL(0, 0, 0, 0)
 HFG_DECL(1, 0, 0, 0)
 HFG_DECL(1, 0, 1, 0)
@@ -31,6 +33,8 @@ HFG_DECL(2, 2, 2, 2)
 #undef HFG_DECL
 
 cudaError_t launch_jk(int la, int lb, int lc, int ld, bool fp32, const JKLaunchArgs& a, cudaStream_t st);
+// The same over several molecules (a.jobs, a.job_steps, a.njobs; RHF).
+cudaError_t launch_jk_batch(int la, int lb, int lc, int ld, bool fp32, const JKLaunchArgs& a, cudaStream_t st);
 cudaError_t launch_schwarz(int la, int lb, const PairInfo* pairs, const PrimPair* prims, int first, int count,
                            const double* boys, const double* expt, double* out, int prim_mode, cudaStream_t st);
 // out[0] += evaluated primitive quartets, out[1] += evaluated shell quartets

@@ -218,27 +218,17 @@ __device__ __forceinline__ T run_sum(T v, int lane, int end) {
   return v;
 }
 
-// A warp takes one bra shell pair and up to 32 ket pairs of one pair class,
-// one shell quartet per lane.
+// One work-queue step of a launch: a warp takes one bra shell pair and up
+// to 32 ket pairs of one pair class per task, one shell quartet per lane.
+// Step c holds tasks [chunk_start[c], chunk_start[c + 1]) and chunk_entry[c]
+// is the entry of its first task; later tasks of the step walk the prefix
+// forward.
 template <int LA, int LB, int LC, int LD, typename T, int NS>
-__global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk_kernel(const JKLaunchArgs a) {
+__device__ __forceinline__ void jk_step(const JKLaunchArgs& a, long long c, int lane, const T* __restrict__ sm) {
   using C = EriClass<LA, LB, LC, LD>;
   constexpr bool SEG = sizeof(T) == 4 ? HFG_JK_SEG_F32 : HFG_JK_SEG_F64;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sm = reinterpret_cast<T*>(smem_raw);
-  boys_stage<T, C::L>(sm, Prec<T>::table(a), Prec<T>::expt(a));
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  // Warp tasks are handed out one work-queue step at a time through the
-  // launch's atomic counter (it counts steps); step c holds tasks
-  // [chunk_start[c], chunk_start[c + 1]) and chunk_entry[c] is the entry of
-  // its first task; later tasks of the step walk the prefix forward.
-  for (;;) {
-    unsigned long long c = 0;
-    if (lane == 0) c = atomicAdd(a.counter, 1ull);
-    c = __shfl_sync(0xffffffffu, c, 0);
-    if ((long long)c >= a.nchunks) break;
+  {
     const long long t0 = __ldg(a.chunk_start + c), t1 = __ldg(a.chunk_start + c + 1);
     int e = __ldg(a.chunk_entry + c);
     long long next = __ldg(a.prefix + e + 1);
@@ -391,6 +381,71 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
         if (lane == 0) atomicAdd(a.Jacc + (size_t)(bra.ao_a + x / NB) * a.n + bra.ao_b + x % NB, (double)v);
       }
     }
+  }
+}
+
+// Persistent blocks: each stages the Boys Taylor rows of its class in shared
+// memory once, then takes work-queue steps from the launch's atomic counter
+// until the launch is done.
+template <int LA, int LB, int LC, int LD, typename T, int NS>
+__global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk_kernel(const JKLaunchArgs a) {
+  using C = EriClass<LA, LB, LC, LD>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  boys_stage<T, C::L>(sm, Prec<T>::table(a), Prec<T>::expt(a));
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(a.counter, 1ull);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if ((long long)c >= a.nchunks) break;
+    jk_step<LA, LB, LC, LD, T, NS>(a, (long long)c, lane, sm);
+  }
+}
+
+// One launch of class (LA LB|LC LD) over the work queues of several
+// molecules (RHF): the launch's steps are the molecules' steps one after
+// another (job_steps[j] is the first step of molecule j), and each step runs
+// with its molecule's pair tables, records, thresholds, density and
+// accumulators.
+template <int LA, int LB, int LC, int LD, typename T>
+__global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk_batch_kernel(const JKLaunchArgs a) {
+  using C = EriClass<LA, LB, LC, LD>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  boys_stage<T, C::L>(sm, Prec<T>::table(a), Prec<T>::expt(a));
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(a.counter, 1ull);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if ((long long)c >= a.nchunks) break;
+    int lo = 0, hi = a.njobs;  // last job whose first step is <= c
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(a.job_steps + mid) <= (long long)c) lo = mid; else hi = mid;
+    }
+    const JKJob& jb = a.jobs[lo];
+    JKLaunchArgs la = a;
+    la.entries = jb.entries;
+    la.prefix = jb.prefix;
+    la.chunk_start = jb.chunk_start;
+    la.chunk_entry = jb.chunk_entry;
+    la.pairs = jb.pairs;
+    la.pairQ = jb.pairQ;
+    la.rec64 = jb.rec64;
+    la.rec32 = jb.rec32;
+    la.pbound = jb.pbound;
+    la.Dtot = jb.Dtot;
+    la.Dspin = jb.Dtot;
+    la.Jacc = jb.Jacc;
+    la.Kacc = jb.Kacc;
+    la.n = jb.n;
+    la.thr = jb.thr;
+    la.prim_eps = jb.prim_eps;
+    jk_step<LA, LB, LC, LD, T, 1>(la, (long long)c - __ldg(a.job_steps + lo), lane, sm);
   }
 }
 

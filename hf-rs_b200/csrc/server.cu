@@ -12,6 +12,16 @@
 // are reported with their submit / start / end times for latency
 // percentiles.  hf-rs has no serving layer; this is the request loop that
 // calls the hf-rs-equivalent SCF entry point for each job.
+//
+// Fock builds of small RHF jobs are batched across jobs: their contexts
+// route every J/K build to the server's batcher, which collects the builds
+// that the running jobs submit within a short window (or until every
+// batching job has one queued) and runs them as one batched build
+// (jk_batch_locked: one launch per angular class over all their work
+// queues).  A small molecule's own build is a few dozen launches of a few
+// blocks each, which leave most of the GPU idle; a batch fills it.  Larger
+// jobs, whose own launches fill the GPU, and UHF jobs build alone on their
+// streams.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -19,6 +29,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -39,10 +50,123 @@ struct JobCopy {
 
 }  // namespace
 
+namespace hfg {
+
+struct JKBatcher {
+  struct Req {
+    hfg_ctx* ctx;
+    hfg_jk_opts o;
+    const double* P;
+    double* J;
+    double* K;
+    int rc;
+    bool done;
+  };
+  int device = 0;
+  double window_us = 300.0;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<Req*> open;  // builds of the batch being collected
+  int participants = 0;    // running jobs whose builds come here
+  long long batches = 0, builds = 0;
+  // one batch enqueues at a time, on the batcher's stream, with its tables
+  // staged through a ring of pinned buffers
+  std::mutex exec_mu;
+  cudaStream_t stream = nullptr;
+  static constexpr int kSlots = 4;
+  static constexpr size_t kSlotBytes = 1 << 20;
+  BatchStaging slots[kSlots];
+  int next_slot = 0;
+
+  explicit JKBatcher(int dev) : device(dev) {
+    cudaSetDevice(dev);
+    cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    for (auto& x : slots) {
+      if (cudaMallocHost(&x.host, kSlotBytes) == cudaSuccess) x.bytes = kSlotBytes; else x.host = nullptr;
+      cudaEventCreateWithFlags(&x.ev, cudaEventDisableTiming);
+    }
+    cudaGetLastError();
+  }
+  ~JKBatcher() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& x : slots) {
+      if (x.host) cudaFreeHost(x.host);
+      if (x.ev) cudaEventDestroy(x.ev);
+    }
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void join() {
+    std::lock_guard<std::mutex> lk(mu);
+    ++participants;
+  }
+  void leave() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      --participants;
+    }
+    cv.notify_all();  // a collecting batch may now be complete
+  }
+};
+
+// The first build of a batch leads it: it waits until every participant has
+// a build queued or the window has passed, takes the queue and enqueues the
+// batch; the others wait until their batch has been enqueued.  Nothing waits
+// on the device here: each context's stream waits for its batch by event.
+int batcher_submit(JKBatcher* b, hfg_ctx* ctx, const hfg_jk_opts& o, const double* dP, double* dJ, double* dK) {
+  JKBatcher::Req r{ctx, o, dP, dJ, dK, HFG_OK, false};
+  std::unique_lock<std::mutex> lk(b->mu);
+  b->open.push_back(&r);
+  if (b->open.size() > 1) {
+    b->cv.notify_all();
+    b->cv.wait(lk, [&] { return r.done; });
+    return r.rc;
+  }
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds((long long)b->window_us);
+  b->cv.wait_until(lk, deadline, [&] { return (int)b->open.size() >= b->participants; });
+  std::vector<JKBatcher::Req*> batch;
+  batch.swap(b->open);
+  lk.unlock();
+  int rc = HFG_OK;
+  {
+    std::lock_guard<std::mutex> ex(b->exec_mu);
+    const int m = (int)batch.size();
+    std::vector<hfg_ctx*> ctxs(m);
+    std::vector<hfg_jk_opts> opts(m);
+    std::vector<const double*> P(m);
+    std::vector<double*> J(m), K(m);
+    for (int j = 0; j < m; ++j) {
+      ctxs[j] = batch[j]->ctx;
+      opts[j] = batch[j]->o;
+      P[j] = batch[j]->P;
+      J[j] = batch[j]->J;
+      K[j] = batch[j]->K;
+    }
+    BatchStaging* slot = &b->slots[b->next_slot];
+    b->next_slot = (b->next_slot + 1) % JKBatcher::kSlots;
+    cudaSetDevice(b->device);
+    rc = jk_batch_locked(ctxs.data(), m, opts.data(), P.data(), J.data(), K.data(), b->stream, slot);
+  }
+  lk.lock();
+  ++b->batches;
+  b->builds += (long long)batch.size();
+  for (JKBatcher::Req* q : batch) {
+    q->rc = rc;
+    q->done = true;
+  }
+  lk.unlock();
+  b->cv.notify_all();
+  return rc;
+}
+
+}  // namespace hfg
+
 struct hfg_server {
   int device = 0;
   long long budget = 0, in_use = 0;
   int mixed_min_ao = 256;  // mixed-precision jobs below this size run FP64
+  int batch_max_ao = 256;  // RHF jobs below this size batch their Fock builds (0: none)
+  std::unique_ptr<hfg::JKBatcher> batcher;
   std::chrono::steady_clock::time_point t0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -110,6 +234,12 @@ void worker(hfg_server* s) {
                 job.coefs.data()};
     hfg_ctx* ctx = nullptr;
     int rc = hfg_ctx_create(&b, s->device, st, &ctx);
+    bool batched = false;
+    if (rc == HFG_OK && !job.spec.uhf && job.n < s->batch_max_ao && s->batcher) {
+      ctx->batcher = s->batcher.get();
+      s->batcher->join();
+      batched = true;
+    }
     if (rc == HFG_OK) {
       hfg_scf_opts o;
       hfg_scf_opts_default(&o);
@@ -141,6 +271,7 @@ void worker(hfg_server* s) {
       r.converged = res.converged;
       r.n_ao = job.n;
     }
+    if (batched) s->batcher->leave();
     if (ctx) hfg_ctx_destroy(ctx);
     cudaStreamSynchronize(st);
     r.status = rc;
@@ -168,6 +299,7 @@ int hfg_server_create(int device, int slots, long long hbm_budget_bytes, hfg_ser
   s->device = device;
   s->budget = hbm_budget_bytes;
   s->t0 = std::chrono::steady_clock::now();
+  s->batcher = std::make_unique<hfg::JKBatcher>(device);
   for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker, s);
   *out = s;
   return HFG_OK;
@@ -215,6 +347,25 @@ int hfg_server_set_mixed_min_ao(hfg_server* s, int n_ao) {
   if (!s || n_ao < 0) return HFG_ERR_INVALID_INPUT;
   std::lock_guard<std::mutex> lk(s->mu);
   s->mixed_min_ao = n_ao;
+  return HFG_OK;
+}
+
+int hfg_server_set_batching(hfg_server* s, int max_ao, double window_us) {
+  if (!s || max_ao < 0 || !(window_us >= 0.0) || window_us > 1e6) return HFG_ERR_INVALID_INPUT;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->batch_max_ao = max_ao;
+  }
+  std::lock_guard<std::mutex> lk(s->batcher->mu);
+  s->batcher->window_us = window_us;
+  return HFG_OK;
+}
+
+int hfg_server_batch_stats(hfg_server* s, long long* batched_builds, long long* batches) {
+  if (!s) return HFG_ERR_INVALID_INPUT;
+  std::lock_guard<std::mutex> lk(s->batcher->mu);
+  if (batched_builds) *batched_builds = s->batcher->builds;
+  if (batches) *batches = s->batcher->batches;
   return HFG_OK;
 }
 

@@ -152,6 +152,7 @@ def load_library():
     L.hfg_jk_device.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
     L.hfg_jk_device_shard.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP, ctypes.c_int, ctypes.c_int]
     L.hfg_jk_device_noalloc.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
+    L.hfg_jk_device_batch.argtypes = [P(VP), ctypes.c_int, P(JKOptions), P(VP), P(VP), P(VP), VP]
     L.hfg_fock_rhf.argtypes = [VP, P(JKOptions), DP, DP, DP]
     L.hfg_fock_uhf.argtypes = [VP, P(JKOptions), DP, DP, DP, DP, DP]
     L.hfg_jk_last_stats.argtypes = [VP, P(JKStats)]
@@ -178,6 +179,8 @@ def load_library():
     L.hfg_server_poll.argtypes = [VP, P(JobResult), ctypes.c_int, P(ctypes.c_int), ctypes.c_int]
     L.hfg_server_stats.argtypes = [VP, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_longlong)]
     L.hfg_server_set_mixed_min_ao.argtypes = [VP, ctypes.c_int]
+    L.hfg_server_set_batching.argtypes = [VP, ctypes.c_int, ctypes.c_double]
+    L.hfg_server_batch_stats.argtypes = [VP, P(ctypes.c_longlong), P(ctypes.c_longlong)]
     L.hfg_server_destroy.argtypes = [VP]
     L.hfg_scf.argtypes = [VP, P(SCFOptions), P(SCFResult), DP, DP, DP, DP]
     _lib = L
@@ -294,6 +297,21 @@ class Context:
         """Device-pointer form (integers); runs on the context stream."""
         o = opts or JKOptions.make()
         self._check(self.lib.hfg_jk_device(self.h, ctypes.byref(o), nspin, d_total, d_spin, d_J, d_K))
+
+    @staticmethod
+    def jk_device_batch(contexts, d_P, d_J, d_K, opts=None, stream=None):
+        """RHF J and K of several molecules in one pass (hfg_jk_device_batch):
+        one context per molecule, device-pointer lists (integers).  Runs on
+        `stream` (None: the first context's stream) and does not synchronise."""
+        m = len(contexts)
+        if not (len(d_P) == len(d_J) == len(d_K) == m) or m == 0:
+            raise ValueError("one density, J and K per context")
+        arr = lambda xs: (VP * m)(*[VP(int(x)) for x in xs])
+        hs = (VP * m)(*[c.h for c in contexts])
+        o = opts or JKOptions.make()
+        c0 = contexts[0]
+        c0._check(c0.lib.hfg_jk_device_batch(hs, m, ctypes.byref(o), arr(d_P), arr(d_J), arr(d_K),
+                                             VP(int(stream) if stream else 0)))
 
     def fock_rhf(self, H, P, opts=None):
         n = self.n
@@ -544,7 +562,10 @@ class DFTensor:
 class Server:
     """hfg_server: continuous admission of SCF jobs onto worker slots."""
 
-    def __init__(self, device=0, slots=8, hbm_budget_bytes=64 << 30, mixed_min_ao=None):
+    def __init__(self, device=0, slots=8, hbm_budget_bytes=64 << 30, mixed_min_ao=None, batch_max_ao=None,
+                 batch_window_us=300.0):
+        """batch_max_ao: RHF jobs below this many functions batch their Fock
+        builds across jobs (0 turns batching off; None keeps the default)."""
         self.lib = load_library()
         h = VP()
         rc = self.lib.hfg_server_create(device, slots, hbm_budget_bytes, ctypes.byref(h))
@@ -553,6 +574,16 @@ class Server:
         self.h = h
         if mixed_min_ao is not None:
             self.lib.hfg_server_set_mixed_min_ao(h, mixed_min_ao)
+        if batch_max_ao is not None:
+            rc = self.lib.hfg_server_set_batching(h, batch_max_ao, batch_window_us)
+            if rc != 0:
+                raise HfgError(rc, "hfg_server_set_batching failed")
+
+    def batch_stats(self):
+        """Fock builds that went through cross-job batches, and batch count."""
+        b, n = ctypes.c_longlong(), ctypes.c_longlong()
+        self.lib.hfg_server_batch_stats(self.h, ctypes.byref(b), ctypes.byref(n))
+        return {"batched_builds": b.value, "batches": n.value}
 
     def submit(self, basis, charge=0, multiplicity=1, uhf=False, spherical=False, tol=1e-10, max_iter=100,
                jk=None, tag=0):

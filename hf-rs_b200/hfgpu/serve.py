@@ -38,11 +38,14 @@ def build_inputs(jobs):
 
 
 def run_stream(jobs, slots, budget_bytes, jk=None, tol=1e-10, honour_arrivals=True, inputs=None, device=0,
-               mixed_min_ao=None):
+               mixed_min_ao=None, batch_max_ao=None, batch_window_us=300.0, stats_out=None):
     """Submit jobs at their arrival times; return per-job results (latency =
-    end - arrival) and the makespan."""
+    end - arrival) and the makespan.  batch_max_ao: the server's cross-job
+    Fock-build batching bound (0: off; None: the server default); stats_out,
+    when a dict, receives the server's batch statistics."""
     inputs = inputs or build_inputs(jobs)
-    srv = Server(device=device, slots=slots, hbm_budget_bytes=budget_bytes, mixed_min_ao=mixed_min_ao)
+    srv = Server(device=device, slots=slots, hbm_budget_bytes=budget_bytes, mixed_min_ao=mixed_min_ao,
+                 batch_max_ao=batch_max_ao, batch_window_us=batch_window_us)
     t0 = time.time()
     submit_wall = {}
     results = []
@@ -61,6 +64,8 @@ def run_stream(jobs, slots, budget_bytes, jk=None, tol=1e-10, honour_arrivals=Tr
             break
         results.extend(got)
     makespan = time.time() - t0
+    if stats_out is not None:
+        stats_out.update(srv.batch_stats())
     srv.close()
     by_tag = {r["tag"]: r for r in results}
     out = []

@@ -151,6 +151,21 @@ int hfg_jk_device(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double
 int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* d_P_total,
                           const double* d_P_spin, double* d_J, double* d_K);
 
+/*
+ * No counterpart in hf-rs, which builds one molecule's J and K per call
+ * (contract_jk, src/scf.rs:337-364).  RHF J and K of n_jobs molecules, one
+ * context each (no context twice, all on one device), in one pass: for each
+ * angular class and precision one launch covers the work queues of every
+ * molecule, so a batch of small molecules fills the GPU where their
+ * separate builds would each leave it mostly idle.  d_P[j], d_J[j], d_K[j]
+ * are molecule j's n_j x n_j device matrices; results equal hfg_jk_device's
+ * per molecule up to FP64 summation order.  Runs on `stream` (NULL: the
+ * first context's stream), after the work already queued on every context
+ * stream, and every context stream waits for it.  Does not synchronise.
+ */
+int hfg_jk_device_batch(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, const double* const* d_P,
+                        double* const* d_J, double* const* d_K, void* stream);
+
 /* Stands in for build_fock_matrix (src/scf.rs:366-369): F = H + J - K/2. */
 int hfg_fock_rhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* P, double* F);
 
@@ -405,6 +420,14 @@ int hfg_server_stats(hfg_server* server, int* pending, int* running, long long* 
    functions run FP64 (primitive screening at 1e-15 at most): on small jobs
    the refinement builds cost more than FP32 saves.  Default 256. */
 int hfg_server_set_mixed_min_ao(hfg_server* server, int n_ao);
+/* Fock builds of RHF jobs with fewer than max_ao functions are batched
+   across the running jobs (hfg_jk_device_batch's launches): a batch takes
+   the builds submitted within window_us of its first one, or fewer when
+   every batching job has one queued.  max_ao = 0 turns batching off.
+   Defaults: 256 functions, 300 us. */
+int hfg_server_set_batching(hfg_server* server, int max_ao, double window_us);
+/* Builds that went through batches, and the number of batches. */
+int hfg_server_batch_stats(hfg_server* server, long long* batched_builds, long long* batches);
 /* Finishes the queued jobs, then stops the workers. */
 int hfg_server_destroy(hfg_server* server);
 

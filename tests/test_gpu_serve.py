@@ -25,8 +25,7 @@ def test_admission_by_footprint_limits_concurrency():
     res, _ = run_stream(jobs, slots=6, budget_bytes=24 << 20, honour_arrivals=False, inputs=inputs)
     # with a 24 MiB budget the jobs (each several MiB) cannot all run at once:
     # some job must start only after another ended
-    starts = sorted((r["start_ms"], r["end_ms"]) for r in res)
-    assert any(s2 >= e1 for (s1, e1), (s2, e2) in zip(starts, starts[1:]))
+    assert any(b["start_ms"] >= a["end_ms"] for a in res for b in res if a is not b)
     assert all(r["status"] == 0 for r in res)
 
 
@@ -46,3 +45,20 @@ def test_mixed_jobs_same_alone_and_in_the_mix_with_arrivals():
         assert abs(a["energy"] - m["energy"]) < 1e-9, (a["tag"], a["energy"], m["energy"])
     # some job was submitted while another was already running
     assert any(o["start_ms"] < m["submit_ms"] < o["end_ms"] for m in mixed for o in mixed if o is not m)
+
+
+def test_batched_fock_builds_match_unbatched_jobs():
+    # RHF jobs below the size bound hand their Fock builds to the server's
+    # batcher, which runs the builds of the running jobs as one batched
+    # build; every converged energy equals the job run alone, unbatched
+    jobs = make_stream(12, rate=1000.0, max_waters=5, seed=23)
+    inputs = build_inputs(jobs)
+    alone, _ = run_stream(jobs, slots=1, budget_bytes=8 << 30, honour_arrivals=False, inputs=inputs, batch_max_ao=0)
+    stats = {}
+    batched, _ = run_stream(jobs, slots=8, budget_bytes=8 << 30, honour_arrivals=False, inputs=inputs,
+                            batch_max_ao=1 << 20, batch_window_us=2000.0, stats_out=stats)
+    assert all(r["status"] == 0 and r["converged"] for r in alone + batched)
+    for a, m in zip(alone, batched):
+        assert abs(a["energy"] - m["energy"]) < 1e-9, (a["tag"], a["energy"], m["energy"])
+    # builds of different jobs shared batches
+    assert stats["batches"] > 0 and stats["batched_builds"] > stats["batches"], stats
