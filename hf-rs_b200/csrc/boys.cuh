@@ -20,8 +20,9 @@
 //    changes F_m by less than 1e-13 relative and is dropped.
 //
 // The FP32 flavour (only for quartets with small Schwarz bounds) uses an
-// order-4 Taylor row F_L/k!, k = 0..4 plus e^{-T0} (T <= 36), __expf, and
-// rsqrtf; its truncation is below 1e-9 relative.
+// order-4 Taylor row F_L/k!, k = 0..4 plus e^{-T0} and __expf for T <= 36
+// (truncation below 1e-9 relative); for T > 36 it evaluates the FP64 branch
+// above and rounds each F_m to FP32.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -110,13 +111,20 @@ __device__ __forceinline__ void boys_eval(double t, const double* __restrict__ s
 template <int L>
 __device__ __forceinline__ void boys_eval(float t, const float* __restrict__ sm, float* F) {
   if (t > 36.0f) {
-    const float r = rsqrtf(t);
-    F[0] = 0.88622692545f * r;
+    // large T in FP64: the asymptotic F_0 and the upward recursion of the
+    // FP64 flavour, rounded to FP32 once per order
+    const double td = t;
+    const double r = rsqrt(td);
+    double f = kHalfSqrtPi * r;
+    F[0] = (float)f;
     if (L > 0) {
-      const float inv2t = 0.5f * r * r;
-      const float e = L <= 2 ? 0.0f : __expf(-t);
+      const double inv2t = 0.5 * r * r;
+      const double e = L <= 2 ? 0.0 : exp(-td);
 #pragma unroll
-      for (int m = 1; m <= L; ++m) F[m] = ((2 * m - 1) * F[m - 1] - e) * inv2t;
+      for (int m = 1; m <= L; ++m) {
+        f = ((2 * m - 1) * f - e) * inv2t;
+        F[m] = (float)f;
+      }
     }
     return;
   }

@@ -646,7 +646,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
       (o.precision != HFG_FP64 && o.precision != HFG_MIXED))
     return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid J/K options");
   // a context served with others hands its RHF builds to their batcher
-  if (ctx->batcher && nspin == 1 && nshards == 1 && dPs == dPt)
+  if (ctx->batcher && nspin == 1 && nshards == 1 && dPs == dPt && !o.deterministic)
     return batcher_submit(ctx->batcher, ctx, o, dPt, dJ, dK);
   Plan* plan = nullptr;
   int rc = build_plan(ctx, o.schwarz_threshold, o.mixed_threshold, o.prim_threshold, o.precision, plan);
@@ -664,7 +664,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   // iteration); the first build of a sequence always runs eagerly, so the
   // kernels' one-time attribute and occupancy set-up happens outside any
   // capture.  Shards and profiled builds run eagerly.
-  const bool graphs_on = ctx->use_graphs && nshards == 1 && !profile;
+  const bool graphs_on = ctx->use_graphs && nshards == 1 && !profile && !o.deterministic;
   const hfg_ctx::GraphKey key{plan, nspin, dPt, dPs, dJ, dK, ctx->d_Jacc.p, ctx->d_Kacc.p, ctx->d_counters.p};
   if (graphs_on) {
     auto it = ctx->graphs.find(key);
@@ -693,6 +693,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   a.n = ctx->n;
   a.nspin = nspin;
   a.prim_eps = o.prim_threshold;
+  a.serial = o.deterministic != 0;
   auto enqueue = [&]() -> int {
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Jacc.p, 0, nn * sizeof(double), ctx->stream));
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Kacc.p, 0, nspin * nn * sizeof(double), ctx->stream));
@@ -710,7 +711,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   // small molecule's build then costs about its slowest class instead of the
   // sum over classes; a large one's persistent grids fill the GPU either way.
   // Profiled builds stay on one stream (per-launch events).
-  const int nstreams = profile ? 1 : 1 + kJKSideStreams;
+  const int nstreams = (profile || a.serial) ? 1 : 1 + kJKSideStreams;
   if (nstreams > 1) {
     HFG_CUDA(ctx, ctx->ensure_side_streams());
     HFG_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
@@ -854,6 +855,7 @@ void hfg_jk_opts_default(hfg_jk_opts* o) {
   o->schwarz_threshold = 1e-12;
   o->prim_threshold = 0.0;
   o->precision = HFG_FP64;
+  o->deterministic = 0;
   o->mixed_threshold = 1e-7;
 }
 

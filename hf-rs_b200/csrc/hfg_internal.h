@@ -94,6 +94,10 @@ struct JKLaunchArgs {
   double* Kacc;        // nspin n x n
   int n, nspin;
   double prim_eps;
+  // deterministic mode: one warp takes the steps in order and each task runs
+  // once per lane with only that lane's quartet active, so every atomic add
+  // lands in a fixed order
+  int serial;
   // batched launches: molecule table and the first step of each molecule
   const JKJob* jobs;
   const long long* job_steps;

@@ -34,6 +34,10 @@ static cudaError_t launch_t(const JKLaunchArgs& a, cudaStream_t st) {
     resident = sms * (per_sm > 0 ? per_sm : 1);
     if (dev >= 0 && dev < kMaxDev) resident_by_dev[dev].store(resident, std::memory_order_relaxed);
   }
+  if (a.serial) {
+    if (a.nchunks > 0) kern<<<1, 32, smem, st>>>(a);
+    return cudaGetLastError();
+  }
   const long long want = (a.nchunks + (block / 32) - 1) / (block / 32);
   const long long grid = want < resident ? want : resident;
   if (grid <= 0) return cudaSuccess;

@@ -232,153 +232,158 @@ __device__ __forceinline__ void jk_step(const JKLaunchArgs& a, long long c, int 
     const long long t0 = __ldg(a.chunk_start + c), t1 = __ldg(a.chunk_start + c + 1);
     int e = __ldg(a.chunk_entry + c);
     long long next = __ldg(a.prefix + e + 1);
+    const int rounds = a.serial ? 32 : 1;
     for (long long warp = t0; warp < t1; ++warp) {
       while (warp >= next) {
         ++e;
         next = a.prefix[e + 1];
       }
-      const JKEntry ent = a.entries[e];
-      const int kidx = ent.k_lo + (int)(warp - a.prefix[e]) * 32 + lane;
-      // kets are bucketed by bound: the exact Schwarz test per quartet
-      const bool active = kidx < ent.k_hi && __ldg(a.pairQ + kidx) * __ldg(a.pairQ + ent.bra) > a.thr;
-      const PairInfo bra = a.pairs[ent.bra];
-      const PairInfo ket = a.pairs[active ? kidx : ent.k_lo];
-      // the next task usually continues this entry: start fetching its ket
-      // pair, and its first primitive records (kets of one class have equal
-      // primitive counts and consecutive records, so they start 32 on)
-      if (HFG_JK_PREFETCH && warp + 1 < t1 && kidx + 32 < ent.k_hi) {
-        prefetch_l1(&a.pairs[kidx + 32]);
-        prefetch_l1(RecOf<T>::get(a) + ket.rec_off + 32);
-        prefetch_l1(a.pbound + ket.rec_off + 32);
-      }
-      T acc[C::NACC];
+      for (int round = 0; round < rounds; ++round) {
+        const JKEntry ent = a.entries[e];
+        const int kidx = ent.k_lo + (int)(warp - a.prefix[e]) * 32 + lane;
+        // kets are bucketed by bound: the exact Schwarz test per quartet (in
+        // deterministic mode, only lane `round`'s quartet this round)
+        const bool active = kidx < ent.k_hi && __ldg(a.pairQ + kidx) * __ldg(a.pairQ + ent.bra) > a.thr &&
+                            (rounds == 1 || lane == round);
+        const PairInfo bra = a.pairs[ent.bra];
+        const PairInfo ket = a.pairs[active ? kidx : ent.k_lo];
+        // the next task usually continues this entry: start fetching its ket
+        // pair, and its first primitive records (kets of one class have equal
+        // primitive counts and consecutive records, so they start 32 on)
+        if (HFG_JK_PREFETCH && warp + 1 < t1 && kidx + 32 < ent.k_hi) {
+          prefetch_l1(&a.pairs[kidx + 32]);
+          prefetch_l1(RecOf<T>::get(a) + ket.rec_off + 32);
+          prefetch_l1(a.pbound + ket.rec_off + 32);
+        }
+        T acc[C::NACC];
 #pragma unroll
-      for (int x = 0; x < C::NACC; ++x) acc[x] = (T)0;
-      if (active) {
-        using Rec = typename RecOf<T>::type;
-        const T ACx = (T)(bra.Ax - ket.Ax), ACy = (T)(bra.Ay - ket.Ay), ACz = (T)(bra.Az - ket.Az);
-        const T bABx = (T)bra.ABx, bABy = (T)bra.ABy, bABz = (T)bra.ABz;
-        const T kABx = (T)ket.ABx, kABy = (T)ket.ABy, kABz = (T)ket.ABz;
-        const Rec* __restrict__ br = RecOf<T>::get(a) + bra.rec_off;
-        const Rec* __restrict__ kr = RecOf<T>::get(a) + ket.rec_off;
-        const float* __restrict__ bb = a.pbound + bra.rec_off;
-        const float* __restrict__ kb = a.pbound + ket.rec_off;
-        const int nb = bra.npp, nk = ket.npp, bs = bra.rec_stride, ks = ket.rec_stride;
-        // screening products in FP32 (bounds are stored as floats; count_kernel
-        // evaluates the same products)
-        const float eps = (float)a.prim_eps;
-        const float bmax = bb[0];
-        // ket primitive pairs while they survive against the largest bra one
-        // (bounds sorted descending); the next record and bound are fetched
-        // one iteration ahead
-        Rec Qn = kr[0];
-        float qbn = kb[0];
-        for (int ik = 0; ik < nk; ++ik) {
-          const Rec Q = Qn;
-          const float qb = qbn;
-          if (qb * bmax < eps) break;
-          if (ik + 1 < nk) {
-            Qn = kr[(ik + 1) * ks];
-            qbn = kb[(ik + 1) * ks];
-          }
-          const T QCx = -Q.bp * kABx, QCy = -Q.bp * kABy, QCz = -Q.bp * kABz;
-          int ib = 0;
-          if constexpr (C::NACC <= 9) {
-            // two independent primitive quartets per step (bra primitive pairs
-            // are sorted by bound: if the second survives, so does the first)
-            for (; ib + 1 < nb; ib += 2) {
-              if (bb[(ib + 1) * bs] * qb < eps) break;
-              const Rec P0 = br[ib * bs], P1 = br[(ib + 1) * bs];
-              prim_quartet<LA, LB, LC, LD, T>(acc, P0.p, P0.inv_p, P0.kp, -P0.bp * bABx, -P0.bp * bABy,
-                                              -P0.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
-              prim_quartet<LA, LB, LC, LD, T>(acc, P1.p, P1.inv_p, P1.kp, -P1.bp * bABx, -P1.bp * bABy,
-                                              -P1.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
+        for (int x = 0; x < C::NACC; ++x) acc[x] = (T)0;
+        if (active) {
+          using Rec = typename RecOf<T>::type;
+          const T ACx = (T)(bra.Ax - ket.Ax), ACy = (T)(bra.Ay - ket.Ay), ACz = (T)(bra.Az - ket.Az);
+          const T bABx = (T)bra.ABx, bABy = (T)bra.ABy, bABz = (T)bra.ABz;
+          const T kABx = (T)ket.ABx, kABy = (T)ket.ABy, kABz = (T)ket.ABz;
+          const Rec* __restrict__ br = RecOf<T>::get(a) + bra.rec_off;
+          const Rec* __restrict__ kr = RecOf<T>::get(a) + ket.rec_off;
+          const float* __restrict__ bb = a.pbound + bra.rec_off;
+          const float* __restrict__ kb = a.pbound + ket.rec_off;
+          const int nb = bra.npp, nk = ket.npp, bs = bra.rec_stride, ks = ket.rec_stride;
+          // screening products in FP32 (bounds are stored as floats; count_kernel
+          // evaluates the same products)
+          const float eps = (float)a.prim_eps;
+          const float bmax = bb[0];
+          // ket primitive pairs while they survive against the largest bra one
+          // (bounds sorted descending); the next record and bound are fetched
+          // one iteration ahead
+          Rec Qn = kr[0];
+          float qbn = kb[0];
+          for (int ik = 0; ik < nk; ++ik) {
+            const Rec Q = Qn;
+            const float qb = qbn;
+            if (qb * bmax < eps) break;
+            if (ik + 1 < nk) {
+              Qn = kr[(ik + 1) * ks];
+              qbn = kb[(ik + 1) * ks];
+            }
+            const T QCx = -Q.bp * kABx, QCy = -Q.bp * kABy, QCz = -Q.bp * kABz;
+            int ib = 0;
+            if constexpr (C::NACC <= 9) {
+              // two independent primitive quartets per step (bra primitive pairs
+              // are sorted by bound: if the second survives, so does the first)
+              for (; ib + 1 < nb; ib += 2) {
+                if (bb[(ib + 1) * bs] * qb < eps) break;
+                const Rec P0 = br[ib * bs], P1 = br[(ib + 1) * bs];
+                prim_quartet<LA, LB, LC, LD, T>(acc, P0.p, P0.inv_p, P0.kp, -P0.bp * bABx, -P0.bp * bABy,
+                                                -P0.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
+                prim_quartet<LA, LB, LC, LD, T>(acc, P1.p, P1.inv_p, P1.kp, -P1.bp * bABx, -P1.bp * bABy,
+                                                -P1.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
+              }
+            }
+            Rec P = br[(ib < nb ? ib : 0) * bs];
+            for (; ib < nb; ++ib) {
+              const Rec Pn = br[(ib + 1 < nb ? ib + 1 : ib) * bs];
+              if (bb[ib * bs] * qb < eps) break;
+              prim_quartet<LA, LB, LC, LD, T>(acc, P.p, P.inv_p, P.kp, -P.bp * bABx, -P.bp * bABy, -P.bp * bABz, Q.p,
+                                              Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
+              P = Pn;
             }
           }
-          Rec P = br[(ib < nb ? ib : 0) * bs];
-          for (; ib < nb; ++ib) {
-            const Rec Pn = br[(ib + 1 < nb ? ib + 1 : ib) * bs];
-            if (bb[ib * bs] * qb < eps) break;
-            prim_quartet<LA, LB, LC, LD, T>(acc, P.p, P.inv_p, P.kp, -P.bp * bABx, -P.bp * bABy, -P.bp * bABz, Q.p,
-                                            Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
-            P = Pn;
-          }
         }
-      }
-      T jab[NAB];
-      T kac[NS][NA * NC], kbc[NS][NB * NC];
-      if (active) {
-        DBlocks<LA, LB, LC, LD, NS, T> dblk;
-        dblk.load(bra, ket, a);
-        T out[C::NOUT];
-        C::hrr(acc, out, (T)bra.ABx, (T)bra.ABy, (T)bra.ABz, (T)ket.ABx, (T)ket.ABy, (T)ket.ABz);
-        T deg = (T)1;
-        if (bra.same) deg *= (T)0.5;
-        if (ket.same) deg *= (T)0.5;
-        if (kidx == ent.bra) deg *= (T)0.5;
-        // scaled in place (a second block-sized array would double the
-        // per-thread footprint of the large classes)
-#pragma unroll
-        for (int i = 0; i < NA; ++i)
-#pragma unroll
-          for (int j = 0; j < NB; ++j)
-#pragma unroll
-            for (int k = 0; k < NC; ++k)
-#pragma unroll
-              for (int l = 0; l < ND; ++l) {
-                const int x = ((i * NB + j) * NC + k) * ND + l;
-                out[x] *= deg * (T)(comp_scale(LA, i) * comp_scale(LB, j) * comp_scale(LC, k) * comp_scale(LD, l));
-              }
-        digest<LA, LB, LC, LD, NS, T, SEG>(out, bra, ket, a, dblk, jab, kac, kbc);
-      } else {
-#pragma unroll
-        for (int x = 0; x < NAB; ++x) jab[x] = (T)0;
-        if (SEG) {
-#pragma unroll
-          for (int sp = 0; sp < NS; ++sp) {
-#pragma unroll
-            for (int x = 0; x < NA * NC; ++x) kac[sp][x] = (T)0;
-#pragma unroll
-            for (int x = 0; x < NB * NC; ++x) kbc[sp][x] = (T)0;
-          }
-        }
-      }
-      if (SEG) {
-        // runs of consecutive lanes whose kets share shell c (first AO
-        // ket.ao_a); inactive lanes form runs of their own
-        const int key = active ? ket.ao_a : -1 - lane;
-        const int prev = __shfl_up_sync(0xffffffffu, key, 1);
-        const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || key != prev);
-        const unsigned later = heads & (0xfffffffeu << lane);
-        const int end = later ? __ffs(later) - 1 : 32;
-        const bool head = (heads >> lane) & 1u;
-        const int n = a.n, i0 = bra.ao_a, j0 = bra.ao_b, k0 = ket.ao_a;
-#pragma unroll
-        for (int sp = 0; sp < NS; ++sp) {
-          double* K = a.Kacc + (size_t)sp * n * n;
+        T jab[NAB];
+        T kac[NS][NA * NC], kbc[NS][NB * NC];
+        if (active) {
+          DBlocks<LA, LB, LC, LD, NS, T> dblk;
+          dblk.load(bra, ket, a);
+          T out[C::NOUT];
+          C::hrr(acc, out, (T)bra.ABx, (T)bra.ABy, (T)bra.ABz, (T)ket.ABx, (T)ket.ABy, (T)ket.ABz);
+          T deg = (T)1;
+          if (bra.same) deg *= (T)0.5;
+          if (ket.same) deg *= (T)0.5;
+          if (kidx == ent.bra) deg *= (T)0.5;
+          // scaled in place (a second block-sized array would double the
+          // per-thread footprint of the large classes)
 #pragma unroll
           for (int i = 0; i < NA; ++i)
 #pragma unroll
-            for (int k = 0; k < NC; ++k) {
-              const T v = run_sum(kac[sp][i * NC + k], lane, end);
-              if (head && active) atomicAdd(K + (size_t)(i0 + i) * n + k0 + k, 2.0 * (double)v);
-            }
+            for (int j = 0; j < NB; ++j)
 #pragma unroll
-          for (int j = 0; j < NB; ++j)
+              for (int k = 0; k < NC; ++k)
 #pragma unroll
-            for (int k = 0; k < NC; ++k) {
-              const T v = run_sum(kbc[sp][j * NC + k], lane, end);
-              if (head && active) atomicAdd(K + (size_t)(j0 + j) * n + k0 + k, 2.0 * (double)v);
+                for (int l = 0; l < ND; ++l) {
+                  const int x = ((i * NB + j) * NC + k) * ND + l;
+                  out[x] *= deg * (T)(comp_scale(LA, i) * comp_scale(LB, j) * comp_scale(LC, k) * comp_scale(LD, l));
+                }
+          digest<LA, LB, LC, LD, NS, T, SEG>(out, bra, ket, a, dblk, jab, kac, kbc);
+        } else {
+#pragma unroll
+          for (int x = 0; x < NAB; ++x) jab[x] = (T)0;
+          if (SEG) {
+#pragma unroll
+            for (int sp = 0; sp < NS; ++sp) {
+#pragma unroll
+              for (int x = 0; x < NA * NC; ++x) kac[sp][x] = (T)0;
+#pragma unroll
+              for (int x = 0; x < NB * NC; ++x) kbc[sp][x] = (T)0;
             }
+          }
         }
-      }
-      // J'[a,b]: the whole warp shares the bra pair
+        if (SEG) {
+          // runs of consecutive lanes whose kets share shell c (first AO
+          // ket.ao_a); inactive lanes form runs of their own
+          const int key = active ? ket.ao_a : -1 - lane;
+          const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+          const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || key != prev);
+          const unsigned later = heads & (0xfffffffeu << lane);
+          const int end = later ? __ffs(later) - 1 : 32;
+          const bool head = (heads >> lane) & 1u;
+          const int n = a.n, i0 = bra.ao_a, j0 = bra.ao_b, k0 = ket.ao_a;
 #pragma unroll
-      for (int x = 0; x < NAB; ++x) {
-        T v = jab[x];
+          for (int sp = 0; sp < NS; ++sp) {
+            double* K = a.Kacc + (size_t)sp * n * n;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (lane == 0) atomicAdd(a.Jacc + (size_t)(bra.ao_a + x / NB) * a.n + bra.ao_b + x % NB, (double)v);
+            for (int i = 0; i < NA; ++i)
+#pragma unroll
+              for (int k = 0; k < NC; ++k) {
+                const T v = run_sum(kac[sp][i * NC + k], lane, end);
+                if (head && active) atomicAdd(K + (size_t)(i0 + i) * n + k0 + k, 2.0 * (double)v);
+              }
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+#pragma unroll
+              for (int k = 0; k < NC; ++k) {
+                const T v = run_sum(kbc[sp][j * NC + k], lane, end);
+                if (head && active) atomicAdd(K + (size_t)(j0 + j) * n + k0 + k, 2.0 * (double)v);
+              }
+          }
+        }
+        // J'[a,b]: the whole warp shares the bra pair
+#pragma unroll
+        for (int x = 0; x < NAB; ++x) {
+          T v = jab[x];
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+          if (lane == 0) atomicAdd(a.Jacc + (size_t)(bra.ao_a + x / NB) * a.n + bra.ao_b + x % NB, (double)v);
+        }
       }
     }
   }

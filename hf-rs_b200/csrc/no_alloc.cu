@@ -128,6 +128,7 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
   a.n = ctx->n;
   a.nspin = nspin;
   a.prim_eps = o.prim_threshold;
+  a.serial = o.deterministic != 0;
   for (size_t l = 0; l < plan.launches.size(); ++l) {
     const hfg::Launch& L = plan.launches[l];
     a.counter = counters + l;

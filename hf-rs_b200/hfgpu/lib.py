@@ -32,14 +32,15 @@ class HfgBasis(ctypes.Structure):
 
 class JKOptions(ctypes.Structure):
     _fields_ = [("schwarz_threshold", ctypes.c_double), ("prim_threshold", ctypes.c_double),
-                ("precision", ctypes.c_int), ("mixed_threshold", ctypes.c_double)]
+                ("precision", ctypes.c_int), ("deterministic", ctypes.c_int), ("mixed_threshold", ctypes.c_double)]
 
     @classmethod
-    def make(cls, schwarz=1e-12, prim=0.0, mixed=None):
+    def make(cls, schwarz=1e-12, prim=0.0, mixed=None, deterministic=False):
         o = cls()
         o.schwarz_threshold = schwarz
         o.prim_threshold = prim
         o.precision = HFG_FP64 if mixed is None else HFG_MIXED
+        o.deterministic = int(bool(deterministic))
         o.mixed_threshold = 0.0 if mixed is None else mixed
         return o
 

@@ -58,13 +58,18 @@ typedef struct {
   double prim_threshold;    /* drop primitive quartets whose Cauchy-Schwarz bound is
                                below this; 0 reproduces hf-rs's quartet set exactly */
   int precision;            /* hfg_precision */
+  int deterministic;        /* 1: bitwise reproducible J/K for debugging (one warp
+                               runs the work queue in order and its lanes add
+                               into J/K one at a time; slow); 0: atomics in
+                               arrival order (default) */
   double mixed_threshold;   /* HFG_MIXED: quartets with Q_ab*Q_cd below this are
                                evaluated in FP32 and accumulated in FP64 */
 } hfg_jk_opts;
 
 typedef struct hfg_ctx hfg_ctx;
 
-/* Default options: Schwarz 1e-12, no primitive screening, FP64. */
+/* Default options: Schwarz 1e-12, no primitive screening, FP64, atomic
+   (not deterministic) accumulation. */
 void hfg_jk_opts_default(hfg_jk_opts* opts);
 
 /*

@@ -223,3 +223,26 @@ def test_graph_replayed_builds_match_eager(monkeypatch):
             Jg, Kg = J.cpu().numpy().copy(), K.cpu().numpy().copy()
             Je, Ke = eager.jk(Ph, opts=opts)
             assert np.max(np.abs(Jg - Je)) < 1e-12 and np.max(np.abs(Kg - Ke[0])) < 1e-12, call
+
+
+@pytest.mark.parametrize("name,nw,mixed", [("cc-pvdz", 1, None), ("sto-3g", 2, None), ("cc-pvdz", 1, 1e-6)])
+def test_deterministic_mode_is_bitwise_reproducible(name, nw, mixed):
+    # the debugging mode: one warp takes the work queue in order and its lanes
+    # add into J'/K' one at a time, so repeated builds agree to the bit; the
+    # atomic mode agrees with it to FP64 summation order
+    ctx = Context(CartesianBasis.build(water_cluster(nw), name))
+    n = ctx.n
+    rng = np.random.default_rng(3)
+    Pa, Pb = (lambda a: a + a.T)(rng.standard_normal((n, n)) * 0.2), (lambda a: a + a.T)(rng.standard_normal((n, n)) * 0.2)
+    det = JKOptions.make(mixed=mixed, deterministic=True)
+    fast = JKOptions.make(mixed=mixed)
+    for spins in ([Pa], [Pa, Pb]):
+        total = sum(spins)
+        J1, K1 = ctx.jk(total, spins, opts=det)
+        J2, K2 = ctx.jk(total, spins, opts=det)
+        assert np.array_equal(J1, J2) and np.array_equal(K1, K2)
+        J3, K3 = ctx.jk(total, spins, opts=fast)
+        scale = max(1.0, np.abs(J3).max())
+        assert np.max(np.abs(J1 - J3)) < 1e-12 * scale
+        assert np.max(np.abs(K1 - K3)) < 1e-12 * scale
+    ctx.close()
