@@ -299,8 +299,16 @@ def run_ours(args):
         # profiler runs: the mixed builds alone, with the thresholds the
         # autotuner picks on this workload
         opt = JKOptions.make(schwarz=SCHWARZ, prim=1e-13, mixed=1e-6)
-        for _ in range(args.warmup + args.steps):
+        last = args.warmup + args.steps - 1
+        for i in range(last + 1):
+            if i == last:
+                # the last build is an NVTX range "jk_build" (ncu --nvtx-include "jk_build/")
+                torch.cuda.synchronize()
+                torch.cuda.nvtx.range_push("jk_build")
             ctx.jk_device(P.data_ptr(), P.data_ptr(), J.data_ptr(), K.data_ptr(), 1, opt)
+            if i == last:
+                torch.cuda.synchronize()
+                torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         if rank == 0:
             print(json.dumps({"jk_only": True, "waters": args.waters, "builds": args.warmup + args.steps}))
@@ -312,9 +320,10 @@ def run_ours(args):
                                    max_energy_error=TUNE_BUDGET, repeats=1)
     if world > 1:
         # every rank must run the same plan: rank 0's choice
-        ch = torch.tensor([opt_mixed.mixed_threshold, opt_mixed.prim_threshold], dtype=torch.float64, device=dev)
+        ch = torch.tensor([opt_mixed.mixed_threshold, opt_mixed.prim_threshold, opt_mixed.tile],
+                          dtype=torch.float64, device=dev)
         torch.distributed.broadcast(ch, 0)
-        opt_mixed = JKOptions.make(schwarz=SCHWARZ, prim=float(ch[1]), mixed=float(ch[0]))
+        opt_mixed = JKOptions.make(schwarz=SCHWARZ, prim=float(ch[1]), mixed=float(ch[0]), tile=int(ch[2]))
     opt_plain = JKOptions.make(schwarz=SCHWARZ)            # the reference's arithmetic in FP64
     opt_fp64 = JKOptions.make(schwarz=SCHWARZ, prim=PRIM)  # FP64 with primitive screening
 
@@ -448,12 +457,12 @@ def run_ours(args):
     scf_waters = args.waters if args.scf_waters < 0 else args.scf_waters
     if world == 1 and scf_waters > 0:
         scfres = measure_scf(scf_waters, ctx if scf_waters == args.waters else None, opt_mixed)
-    mt, pt = opt_mixed.mixed_threshold, opt_mixed.prim_threshold
+    mt, pt, tl = opt_mixed.mixed_threshold, opt_mixed.prim_threshold, opt_mixed.tile or 64
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_mixed / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64/f32-mixed", "data": "synthetic",
             "config": {"workload": workload(args.waters, n) + ", mixed precision (FP32 below Q_ab*Q_cd < %g, "
-                                   "primitive screening %g; autotuned)" % (mt, pt),
+                                   "primitive screening %g, quartet tile %d; autotuned)" % (mt, pt, tl),
                        "n_ao": n, "waters": args.waters, "parallelism": ("%d shards + NCCL all-reduce of J, K" % world) if world > 1 else "single",
                        "density": "SCF density after 3 iterations from the SAD guess",
                        "l2": "flushed (256 MB write) before every timed step"},
@@ -465,7 +474,7 @@ def run_ours(args):
             "fp64": {"value": value_fp64, "unit": UNIT, "ms_per_step": tot_fp64 / args.steps,
                      "form": "FP64 with primitive screening %g" % PRIM, "wmd_flops": stats_fp64["wmd_flops_fp64"]},
             "mixed_over_fp64_plain": value / value_plain, "mixed_over_fp64": value / value_fp64,
-            "autotune": {"chosen": {"fp32_threshold": mt, "prim_threshold": pt}, "budget_eh": TUNE_BUDGET,
+            "autotune": {"chosen": {"fp32_threshold": mt, "prim_threshold": pt, "tile": tl}, "budget_eh": TUNE_BUDGET,
                          "candidates": tune["candidates"]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck, "serving": serving, "df": dfres,
             "scf": scfres,

@@ -28,7 +28,7 @@
 
 namespace hfg {
 
-constexpr int kBoysCols = 16;   // F_0 .. F_15 per grid point in the global table (L <= 8)
+constexpr int kBoysCols = 24;   // F_0 .. F_23 per grid point in the global table (L <= 16 with order 7)
 constexpr int kBoysRows = 1002; // T in [0, 50.05]
 constexpr double kBoysStep = 0.05;
 constexpr int kBoysSmemRows = 721;  // T <= 36

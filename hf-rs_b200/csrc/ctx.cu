@@ -12,6 +12,7 @@
 #include <numeric>
 
 #include "boys.cuh"
+#include "eri_md.h"
 #include "hfg_ctx.h"
 #include "jk_dispatch.h"
 
@@ -163,6 +164,7 @@ int build_shell_list(hfg_ctx* ctx, const hfg_basis* b, int lmax) {
       }
     }
     ctx->shells.push_back(sh);
+    ctx->lmax = std::max(ctx->lmax, l);
     start += cnt;
   }
   return HFG_OK;
@@ -361,8 +363,10 @@ static int build_pairs(hfg_ctx* ctx) {
 // pair of pair classes (bra class >= ket class) and every bra pair, the
 // significant kets form a prefix of the ket class (kets sorted by Q); in
 // mixed precision the kets below the FP32 threshold form the tail of it.
-static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, int precision, Plan*& out) {
-  auto key = std::make_tuple(thr, precision == HFG_MIXED ? mixed : 0.0, prim_eps, precision);
+static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, int precision, int tile,
+                      Plan*& out) {
+  if (tile <= 0) tile = 64;
+  auto key = std::make_tuple(thr, precision == HFG_MIXED ? mixed : 0.0, prim_eps, precision, tile);
   auto it = ctx->plans.find(key);
   if (it != ctx->plans.end()) {
     out = it->second.get();
@@ -407,7 +411,9 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
         if (cb == ck) nsig = std::min(nsig, i - B.first + 1);
         if (nsig <= 0) continue;
         int n64 = nsig;
-        if (precision == HFG_MIXED) {
+        // classes with an f shell run on the generic engine, FP64 only
+        const bool generic = B.la > kLMax || B.lb > kLMax || Kc.la > kLMax || Kc.lb > kLMax;
+        if (precision == HFG_MIXED && !generic) {
           // FP32 only for buckets whose every ket has qi * qj < mixed
           int jm = 0;
           while (jm < nb && qi * Kc.bqmax[jm] >= mixed) ++jm;
@@ -449,9 +455,10 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     // their warp tasks (bra x ket primitive pairs, before primitive
     // screening), most expensive first, so that the cheap tasks form the
     // tail of the launch; consecutive tasks are cut into steps of about equal
-    // nominal cost (about eight per resident warp, up to 32 warps per SM) and
-    // at most 64 tasks.  Each step's first task and its entry are tabulated,
-    // so no warp searches the prefix.
+    // nominal cost and at most `tile` tasks (the quartet tile: at the
+    // default 64, about eight steps per resident warp, up to 32 warps per
+    // SM; the step cost scales with the tile).  Each step's first task and
+    // its entry are tabulated, so no warp searches the prefix.
     std::vector<double> cost;
     {
       const size_t ne = L.entries.size();
@@ -478,7 +485,7 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
     {
       double total = 0.0;
       for (size_t e = 0; e < L.entries.size(); ++e) total += cost[e] * (double)(L.prefix[e + 1] - L.prefix[e]);
-      const double target = total / ((double)sms * 32 * 8);
+      const double target = total / ((double)sms * 32 * 8) * ((double)tile / 64.0);
       size_t e = 0;
       long long t = 0;
       L.cost_prefix.assign(1, 0.0);
@@ -489,7 +496,7 @@ static int build_plan(hfg_ctx* ctx, double thr, double mixed, double prim_eps, i
         double acc = 0.0;
         long long k = 0;
         size_t ee = e;
-        while (t < nw_total && k < 64 && (k == 0 || acc < target)) {
+        while (t < nw_total && k < tile && (k == 0 || acc < target)) {
           while (L.prefix[ee + 1] <= t) ++ee;
           acc += cost[ee];
           ++t;
@@ -643,13 +650,13 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   if (opts) o = *opts; else hfg_jk_opts_default(&o);
   if (nspin < 1 || nspin > 2) return set_error(ctx, HFG_ERR_INVALID_INPUT, "nspin must be 1 or 2");
   if (!(o.schwarz_threshold >= 0.0) || !(o.prim_threshold >= 0.0) ||
-      (o.precision != HFG_FP64 && o.precision != HFG_MIXED))
+      (o.precision != HFG_FP64 && o.precision != HFG_MIXED) || o.tile < 0 || o.tile > 4096)
     return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid J/K options");
   // a context served with others hands its RHF builds to their batcher
   if (ctx->batcher && nspin == 1 && nshards == 1 && dPs == dPt && !o.deterministic)
     return batcher_submit(ctx->batcher, ctx, o, dPt, dJ, dK);
   Plan* plan = nullptr;
-  int rc = build_plan(ctx, o.schwarz_threshold, o.mixed_threshold, o.prim_threshold, o.precision, plan);
+  int rc = build_plan(ctx, o.schwarz_threshold, o.mixed_threshold, o.prim_threshold, o.precision, o.tile, plan);
   if (rc != HFG_OK) return rc;
   const size_t nn = (size_t)ctx->n * ctx->n;
   HFG_CUDA(ctx, ctx->d_Jacc.alloc(nn));
@@ -857,6 +864,7 @@ void hfg_jk_opts_default(hfg_jk_opts* o) {
   o->precision = HFG_FP64;
   o->deterministic = 0;
   o->mixed_threshold = 1e-7;
+  o->tile = 0;
 }
 
 int hfg_ctx_create(const hfg_basis* basis, int device, void* stream, hfg_ctx** out) {
@@ -887,7 +895,8 @@ int hfg_ctx_create(const hfg_basis* basis, int device, void* stream, hfg_ctx** o
       });
   }
   AllocScope alloc_scope(rc == HFG_OK ? ctx->stream : nullptr);
-  if (rc == HFG_OK) rc = build_shell_list(ctx.get(), basis, kLMax);
+  // s, p, d on the generated kernels; f on the generic engine
+  if (rc == HFG_OK) rc = build_shell_list(ctx.get(), basis, kMDLMax);
   if (rc == HFG_OK) {
     const auto& t = boys_table_host();
     std::vector<float> tf(t.begin(), t.end());
@@ -1086,8 +1095,9 @@ int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, c
     const hfg_jk_opts& o = opts[j];
     if (!d_P[j] || !d_J[j] || !d_K[j]) return fail(HFG_ERR_INVALID_INPUT, "null pointer");
     if (ctxs[j]->device != c0->device) return fail(HFG_ERR_INVALID_INPUT, "the contexts of a batch must share one device");
+    if (ctxs[j]->lmax > kLMax) return fail(HFG_ERR_UNSUPPORTED, "batched builds cover s, p and d shells");
     if (!(o.schwarz_threshold >= 0.0) || !(o.prim_threshold >= 0.0) ||
-        (o.precision != HFG_FP64 && o.precision != HFG_MIXED))
+        (o.precision != HFG_FP64 && o.precision != HFG_MIXED) || o.tile < 0 || o.tile > 4096)
       return fail(HFG_ERR_INVALID_INPUT, "invalid J/K options");
   }
   // per molecule: its plan (built once, cached on its context) and its
@@ -1098,7 +1108,8 @@ int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, c
     hfg_ctx* c = ctxs[j];
     AllocScope alloc_scope(c->stream);
     const hfg_jk_opts& o = opts[j];
-    const int rc = build_plan(c, o.schwarz_threshold, o.mixed_threshold, o.prim_threshold, o.precision, plans[j]);
+    const int rc =
+        build_plan(c, o.schwarz_threshold, o.mixed_threshold, o.prim_threshold, o.precision, o.tile, plans[j]);
     if (rc != HFG_OK) return fail(rc, c->err);
     const size_t nn = (size_t)c->n * c->n;
     BK(c->d_Jacc.alloc(nn));
@@ -1265,10 +1276,16 @@ int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len) {
     return set_error(ctx, HFG_ERR_INVALID_INPUT, "packed length must be n_p (n_p + 1) / 2 with n_p = n (n + 1) / 2");
   if (!(thr >= 0.0)) return set_error(ctx, HFG_ERR_INVALID_INPUT, "Schwarz threshold must be >= 0");
   Plan* plan = nullptr;
-  int rc = build_plan(ctx, thr, 0.0, 0.0, HFG_FP64, plan);
+  int rc = build_plan(ctx, thr, 0.0, 0.0, HFG_FP64, 0, plan);
   if (rc != HFG_OK) return rc;
   HFG_CUDA(ctx, cudaMemsetAsync(d_out, 0, len * sizeof(double), ctx->stream));
   for (const Launch& L : plan->launches) {
+    if (L.la > kLMax || L.lb > kLMax || L.lc > kLMax || L.ld > kLMax) {
+      HFG_CUDA(ctx, launch_eri_packed_md(L.la, L.lb, L.lc, L.ld, L.d_entries, L.d_prefix, (int)L.prefix[0],
+                                         L.prefix[1], ctx->d_pairs.p, ctx->d_pairQ.p, thr, ctx->d_rec64.p,
+                                         ctx->d_pbound.p, ctx->d_boys64.p, ctx->d_expt64.p, d_out, ctx->stream));
+      continue;
+    }
     HFG_CUDA(ctx, launch_eri_packed(L.la, L.lb, L.lc, L.ld, L.d_entries, L.d_prefix, (int)L.prefix[0], L.prefix[1],
                                     ctx->d_pairs.p, ctx->d_pairQ.p, thr, ctx->d_rec64.p, ctx->d_boys64.p, ctx->d_expt64.p, d_out,
                                     ctx->stream));
@@ -1365,6 +1382,9 @@ void hfg_autotune_opts_default(hfg_autotune_opts* o) {
   o->n_prim = 3;
   o->max_energy_error = 5e-9;
   o->repeats = 2;
+  o->tiles[0] = 16;
+  o->tiles[1] = 256;
+  o->n_tile = 2;
 }
 
 int hfg_jk_autotune(hfg_ctx* ctx, const hfg_jk_opts* base, int nspin, const double* dPt, const double* dPs,
@@ -1387,7 +1407,14 @@ int hfg_jk_autotune(hfg_ctx* ctx, const hfg_jk_opts* base, int nspin, const doub
     }
     if (opts->max_energy_error > 0.0) o.max_energy_error = opts->max_energy_error;
     if (opts->repeats > 0) o.repeats = opts->repeats;
+    if (opts->n_tile < 0 || opts->n_tile > 4) return set_error(ctx, HFG_ERR_INVALID_INPUT, "at most 4 tiles");
+    if (opts->n_tile > 0) {
+      o.n_tile = opts->n_tile;
+      for (int i = 0; i < o.n_tile; ++i) o.tiles[i] = opts->tiles[i];
+    }
   }
+  for (int i = 0; i < o.n_tile; ++i)
+    if (o.tiles[i] < 1 || o.tiles[i] > 4096) return set_error(ctx, HFG_ERR_INVALID_INPUT, "tiles must be in 1..4096");
   hfg_jk_opts b;
   if (base) b = *base; else hfg_jk_opts_default(&b);
   std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1470,6 +1497,26 @@ int hfg_jk_autotune(hfg_ctx* ctx, const hfg_jk_opts* base, int nspin, const doub
         res->found = 1;
       }
     }
+  // the quartet tile, on the best threshold pair
+  if (res->found) {
+    const hfg_jk_opts pair = res->best;
+    for (int i = 0; i < o.n_tile && k < 64; ++i, ++k) {
+      hfg_jk_opts c = pair;
+      c.tile = o.tiles[i];
+      double ms = 0.0, dE = 0.0;
+      rc = run(c, J.p, K.p, o.repeats, ms);
+      if (rc != HFG_OK) return rc;
+      rc = energy_error(dE);
+      if (rc != HFG_OK) return rc;
+      res->ms[k] = ms;
+      res->energy_error[k] = dE;
+      if (std::fabs(dE) <= o.max_energy_error && ms < res->best_ms) {
+        res->best = c;
+        res->best_ms = ms;
+        res->best_energy_error = dE;
+      }
+    }
+  }
   res->evaluated = k;
   if (!res->found) res->best_ms = res->fp64_ms;
   return HFG_OK;

@@ -46,6 +46,9 @@ struct AuxSet {
 
 int make_aux_set(hfg_ctx* ctx, const hfg_basis* aux, AuxSet& ax) {
   cudaStream_t st = ctx->stream;
+  // the three-centre kernels cover orbital pairs of s, p and d shells
+  if (ctx->lmax > kLMax)
+    return set_error(ctx, HFG_ERR_UNSUPPORTED, "density fitting covers orbital s, p and d shells");
   int rc = build_shell_list(&ax.shells, aux, 4);
   if (rc != HFG_OK) return set_error(ctx, rc, "auxiliary basis: " + ax.shells.err);
   std::vector<PairInfo> upairs(ax.shells.shells.size());

@@ -133,7 +133,8 @@ struct hfg_ctx {
   std::mutex mu;
   std::string err;
 
-  int n = 0;  // Cartesian functions
+  int n = 0;     // Cartesian functions
+  int lmax = 0;  // highest shell angular momentum
   std::vector<hfg::Shell> shells;
   std::vector<double> exps, coefs;
   std::vector<std::pair<int, int>> ref_pairs;  // hf-rs order: (a, b), a >= b
@@ -161,7 +162,8 @@ struct hfg_ctx {
   hfg::DevBuf<unsigned long long> d_counters;  // one work-queue counter per J/K launch
   hfg::DevBuf<double> d_D, d_Ds, d_Jacc, d_Kacc, d_J, d_K, d_tmp;
 
-  std::map<std::tuple<double, double, double, int>, std::unique_ptr<hfg::Plan>> plans;
+  // launch plans by (Schwarz, FP32 and primitive thresholds, precision, tile)
+  std::map<std::tuple<double, double, double, int, int>, std::unique_ptr<hfg::Plan>> plans;
   hfg_jk_stats last{};
 
   ~hfg_ctx();

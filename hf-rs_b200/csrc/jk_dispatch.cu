@@ -1,10 +1,16 @@
-// Dispatch tables for the J/K, Schwarz and single-quartet kernels.
+// Dispatch tables for the J/K, Schwarz and single-quartet kernels: the
+// generated kernels for s, p and d, the generic engine (eri_md.cu) for
+// classes with an f shell.
 #include "jk_dispatch.h"
+#include "eri_md.h"
 #include "eri_prim.cuh"
 
 namespace hfg {
 
 cudaError_t launch_jk(int la, int lb, int lc, int ld, bool fp32, const JKLaunchArgs& a, cudaStream_t st) {
+  // classes with an f shell: the generic engine, FP64 only
+  if (la > kLMax || lb > kLMax || lc > kLMax || ld > kLMax)
+    return fp32 ? cudaErrorInvalidValue : launch_jk_md(la, lb, lc, ld, a, st);
 #define HFG_CASE(A, B, C, D) \
   if (la == A && lb == B && lc == C && ld == D) return launch_jk_##A##B##C##D(a, fp32, st);
   HFG_CASE(0, 0, 0, 0)
@@ -33,6 +39,7 @@ cudaError_t launch_jk(int la, int lb, int lc, int ld, bool fp32, const JKLaunchA
 }
 
 cudaError_t launch_jk_batch(int la, int lb, int lc, int ld, bool fp32, const JKLaunchArgs& a, cudaStream_t st) {
+  if (la > kLMax || lb > kLMax || lc > kLMax || ld > kLMax) return cudaErrorInvalidValue;
 #define HFG_CASE(A, B, C, D) \
   if (la == A && lb == B && lc == C && ld == D) return launch_jkb_##A##B##C##D(a, fp32, st);
   HFG_CASE(0, 0, 0, 0)
@@ -63,6 +70,7 @@ cudaError_t launch_jk_batch(int la, int lb, int lc, int ld, bool fp32, const JKL
 cudaError_t launch_schwarz(int la, int lb, const PairInfo* pairs, const PrimPair* prims, int first, int count,
                            const double* boys, const double* expt, double* out, int prim_mode, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
+  if (la > kLMax || lb > kLMax) return launch_schwarz_md(la, lb, pairs, prims, first, count, boys, expt, out, prim_mode, st);
   const int smem = (int)boys_smem_bytes<double>();
   const int block = 64, grid = (count + block - 1) / block;
 #define HFG_CASE(A, B)                                                                             \
@@ -83,6 +91,8 @@ cudaError_t launch_schwarz(int la, int lb, const PairInfo* pairs, const PrimPair
 
 cudaError_t launch_quartet(int la, int lb, int lc, int ld, const PairInfo* pairs, const PrimPair* prims,
                            const double* boys, const double* expt, double* out, cudaStream_t st) {
+  if (la > kLMax || lb > kLMax || lc > kLMax || ld > kLMax)
+    return launch_quartet_md(la, lb, lc, ld, pairs, prims, boys, expt, out, st);
   const int smem = (int)boys_smem_bytes<double>();
 #define HFG_CASE(A, B, C, D)                                                    \
   if (la == A && lb == B && lc == C && ld == D) {                               \

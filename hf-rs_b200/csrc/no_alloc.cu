@@ -78,7 +78,7 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
   // would break the ordering of the plan map)
   if (!(o.schwarz_threshold >= 0.0) || !(o.prim_threshold >= 0.0) ||
       (o.precision != HFG_FP64 && o.precision != HFG_MIXED) ||
-      (o.precision == HFG_MIXED && !(o.mixed_threshold >= 0.0)))
+      (o.precision == HFG_MIXED && !(o.mixed_threshold >= 0.0)) || o.tile < 0 || o.tile > 4096)
     return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid J/K options");
   const size_t nn = (size_t)ctx->n * ctx->n;
   const char* too_big =
@@ -88,7 +88,7 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
     return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, too_big);
   std::lock_guard<std::mutex> lk(ctx->mu);
   auto it = ctx->plans.find(std::make_tuple(o.schwarz_threshold, o.precision == HFG_MIXED ? o.mixed_threshold : 0.0,
-                                            o.prim_threshold, o.precision));
+                                            o.prim_threshold, o.precision, o.tile > 0 ? o.tile : 64));
   if (it == ctx->plans.end())
     return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT,
                           "hfg_jk_device_noalloc: no launch plan for these options on this context; call hfg_jk or "

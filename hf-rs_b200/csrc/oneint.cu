@@ -5,7 +5,8 @@
 // mu >= nu, looping over primitive pairs; Hermite expansion coefficients
 // E_t^{ij} per axis, S = E_0^x E_0^y E_0^z (pi/p)^{3/2}, T from the overlap
 // recursion with lb +- 2, V = -Z 2pi/p sum E_t E_u E_v R_tuv(p, P - C) over
-// nuclei.  Written for l <= 2 per shell (lb + 2 <= 4 in the kinetic term).
+// nuclei.  Instantiated for shells up to d (LM = 2) and up to f (LM = 3);
+// the kinetic term needs E up to lb + 2.
 #include <cuda_runtime.h>
 
 #include "boys.cuh"
@@ -13,10 +14,13 @@
 
 namespace hfg {
 
-constexpr int kMaxL1e = 2;
-constexpr int kEI = kMaxL1e + 1;      // i index 0..2
-constexpr int kEJ = kMaxL1e + 3;      // j index 0..4 (lb + 2)
-constexpr int kET = 2 * kMaxL1e + 3;  // t index 0..6
+// Hermite table extents for shells up to angular momentum LM
+template <int LM> struct OneIntDims {
+  static constexpr int EI = LM + 1;      // i index 0..LM
+  static constexpr int EJ = LM + 3;      // j index 0..LM+2 (lb + 2)
+  static constexpr int ET = 2 * LM + 3;  // t index
+  static constexpr int L = 2 * LM;       // highest Boys order of V
+};
 
 struct FuncInfo {
   double c[3];
@@ -38,8 +42,10 @@ struct OneIntArgs {
 };
 
 // E[i][j][t] for one axis, i <= la, j <= lb (+2 allowed), 1D MD recursion.
+template <int LM>
 __device__ __forceinline__ void hermite_1d(int la, int lb, double alpha, double beta, double a, double b,
-                                           double E[kEI][kEJ][kET]) {
+                                           double E[OneIntDims<LM>::EI][OneIntDims<LM>::EJ][OneIntDims<LM>::ET]) {
+  constexpr int kET = OneIntDims<LM>::ET;
   const double p = alpha + beta, inv2p = 0.5 / p;
   const double P = (alpha * a + beta * b) / p;
   const double xpa = P - a, xpb = P - b;
@@ -68,17 +74,20 @@ __device__ __forceinline__ void hermite_1d(int la, int lb, double alpha, double 
 }
 
 __device__ __forceinline__ double comp_norm(const int l[3]) {
-  // 1/sqrt(prod (2 l_i - 1)!!) for l_i <= 2
+  // 1/sqrt(prod (2 l_i - 1)!!)
   double d = 1.0;
   for (int k = 0; k < 3; ++k)
-    if (l[k] == 2) d *= 3.0;
+    for (int m = 2 * l[k] - 1; m > 1; m -= 2) d *= m;
   return rsqrt(d);
 }
 
+template <int LM>
 __global__ void __launch_bounds__(128) oneint_kernel(const OneIntArgs a) {
+  using Dm = OneIntDims<LM>;
+  constexpr int kEI = Dm::EI, kEJ = Dm::EJ, kET = Dm::ET, kL = Dm::L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* sm = reinterpret_cast<double*>(smem_raw);
-  boys_stage<double, 4>(sm, a.boys, a.expt);
+  boys_stage<double, kL>(sm, a.boys, a.expt);
   __syncthreads();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long npair = (long long)a.n * (a.n + 1) / 2;
@@ -98,9 +107,9 @@ __global__ void __launch_bounds__(128) oneint_kernel(const OneIntArgs a) {
       const double al = a.exps[pa + i], be = a.exps[pb + j];
       const double cc = a.coefs[pa + i] * a.coefs[pb + j] * na * nb;
       const double p = al + be, inv_p = 1.0 / p;
-      hermite_1d(A.l[0], B.l[0] + 2, al, be, A.c[0], B.c[0], Ex);
-      hermite_1d(A.l[1], B.l[1] + 2, al, be, A.c[1], B.c[1], Ey);
-      hermite_1d(A.l[2], B.l[2] + 2, al, be, A.c[2], B.c[2], Ez);
+      hermite_1d<LM>(A.l[0], B.l[0] + 2, al, be, A.c[0], B.c[0], Ex);
+      hermite_1d<LM>(A.l[1], B.l[1] + 2, al, be, A.c[1], B.c[1], Ey);
+      hermite_1d<LM>(A.l[2], B.l[2] + 2, al, be, A.c[2], B.c[2], Ez);
       const double pref = 5.56832799683170784528 * inv_p * sqrt(inv_p);  // (pi/p)^{3/2}
       const double sx = Ex[A.l[0]][B.l[0]][0], sy = Ey[A.l[1]][B.l[1]][0], sz = Ez[A.l[2]][B.l[2]][0];
       S += cc * pref * sx * sy * sz;
@@ -120,10 +129,10 @@ __global__ void __launch_bounds__(128) oneint_kernel(const OneIntArgs a) {
       for (int at = 0; at < a.natom; ++at) {
         const double PC[3] = {P[0] - a.atoms[4 * at], P[1] - a.atoms[4 * at + 1], P[2] - a.atoms[4 * at + 2]};
         const double T = p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
-        double F[5];
-        boys_eval<4>(T, sm, F);
+        double F[kL + 1];
+        boys_eval<kL>(T, sm, F);
         // R^n_{tuv} for t+u+v <= L via the MD recursion, n <= L
-        double R[5][5][5][5];  // [n][t][u][v]
+        double R[kL + 1][kL + 1][kL + 1][kL + 1];  // [n][t][u][v]
         double m2p = 1.0;
         for (int n = 0; n <= L; ++n) {
           R[n][0][0][0] = m2p * F[n];
@@ -220,8 +229,9 @@ int one_electron(hfg_ctx* ctx, int natom, const double* pos, const double* charg
   OneIntArgs a{df.p, dex.p, dco.p, doff.p, dK.p, dat.p, natom, n, ctx->d_boys64.p, ctx->d_expt64.p, dS, dT, dV};
   const long long npair = (long long)n * (n + 1) / 2;
   const int smem = (int)boys_smem_bytes<double>();
-  chk(cudaFuncSetAttribute(oneint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "attr");
-  if (npair > 0) oneint_kernel<<<(unsigned)((npair + 127) / 128), 128, smem, ctx->stream>>>(a);
+  auto kern = ctx->lmax <= 2 ? oneint_kernel<2> : oneint_kernel<3>;
+  chk(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "attr");
+  if (npair > 0) kern<<<(unsigned)((npair + 127) / 128), 128, smem, ctx->stream>>>(a);
   chk(cudaGetLastError(), "oneint kernel");
   chk(cudaStreamSynchronize(ctx->stream), "oneint sync");
   return rc;

@@ -301,8 +301,15 @@ int scf_setup(hfg_ctx* ctx, const hfg_scf_opts* o, Scf& s, int& m_out) {
         for (int r = 0; r < cnt; ++r) Tm[(size_t)col++ * n + sh.ao + r] = 1.0;
         continue;
       }
+      // Cartesian components in hf-rs order (d: xx, yy, zz, xy, xz, yz; f and
+      // above lexicographic, src/basis.rs:418-445)
       std::vector<std::array<int, 3>> comps;
-      if (sh.l == 2) comps = {{2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+      if (sh.l == 2) {
+        comps = {{2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+      } else {
+        for (int lx = sh.l; lx >= 0; --lx)
+          for (int ly = sh.l - lx; ly >= 0; --ly) comps.push_back({lx, ly, sh.l - lx - ly});
+      }
       for (int mm = -sh.l; mm <= sh.l; ++mm) {
         solid_harmonic(sh.l, mm, poly);
         std::vector<double> c(cnt, 0.0);

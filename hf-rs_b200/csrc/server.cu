@@ -235,7 +235,7 @@ void worker(hfg_server* s) {
     hfg_ctx* ctx = nullptr;
     int rc = hfg_ctx_create(&b, s->device, st, &ctx);
     bool batched = false;
-    if (rc == HFG_OK && !job.spec.uhf && job.n < s->batch_max_ao && s->batcher) {
+    if (rc == HFG_OK && !job.spec.uhf && job.n < s->batch_max_ao && s->batcher && ctx->lmax <= hfg::kLMax) {
       ctx->batcher = s->batcher.get();
       s->batcher->join();
       batched = true;

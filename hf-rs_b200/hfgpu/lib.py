@@ -32,16 +32,18 @@ class HfgBasis(ctypes.Structure):
 
 class JKOptions(ctypes.Structure):
     _fields_ = [("schwarz_threshold", ctypes.c_double), ("prim_threshold", ctypes.c_double),
-                ("precision", ctypes.c_int), ("deterministic", ctypes.c_int), ("mixed_threshold", ctypes.c_double)]
+                ("precision", ctypes.c_int), ("deterministic", ctypes.c_int), ("mixed_threshold", ctypes.c_double),
+                ("tile", ctypes.c_int)]
 
     @classmethod
-    def make(cls, schwarz=1e-12, prim=0.0, mixed=None, deterministic=False):
+    def make(cls, schwarz=1e-12, prim=0.0, mixed=None, deterministic=False, tile=0):
         o = cls()
         o.schwarz_threshold = schwarz
         o.prim_threshold = prim
         o.precision = HFG_FP64 if mixed is None else HFG_MIXED
         o.deterministic = int(bool(deterministic))
         o.mixed_threshold = 0.0 if mixed is None else mixed
+        o.tile = tile
         return o
 
     def as_dict(self):
@@ -107,7 +109,8 @@ class JKStats(ctypes.Structure):
 class AutotuneOptions(ctypes.Structure):
     _fields_ = [("fp32_thresholds", ctypes.c_double * 8), ("n_fp32", ctypes.c_int),
                 ("prim_thresholds", ctypes.c_double * 8), ("n_prim", ctypes.c_int),
-                ("max_energy_error", ctypes.c_double), ("repeats", ctypes.c_int)]
+                ("max_energy_error", ctypes.c_double), ("repeats", ctypes.c_int),
+                ("tiles", ctypes.c_int * 4), ("n_tile", ctypes.c_int)]
 
 
 class AutotuneResult(ctypes.Structure):
@@ -424,11 +427,17 @@ class Context:
         self._check(self.lib.hfg_jk_last_stats(self.h, ctypes.byref(s)))
         return s.as_dict()
 
-    def autotune(self, d_total, d_spin, nspin=1, base=None, fp32=(), prim=(), max_energy_error=None, repeats=None):
+    def autotune(self, d_total, d_spin, nspin=1, base=None, fp32=(), prim=(), max_energy_error=None, repeats=None,
+                 tiles=None):
         """hfg_jk_autotune on device densities (integer pointers): returns the
-        chosen JKOptions and a report of every candidate."""
+        chosen JKOptions and a report of every candidate.  tiles: quartet
+        tiles tried on the best threshold pair (None: the library's)."""
         o = AutotuneOptions()
         self.lib.hfg_autotune_opts_default(ctypes.byref(o))
+        if tiles is not None:
+            o.n_tile = len(tiles)
+            for i, v in enumerate(tiles):
+                o.tiles[i] = v
         if fp32:
             o.n_fp32 = len(fp32)
             for i, v in enumerate(fp32):
@@ -449,6 +458,9 @@ class Context:
         pl = [o.prim_thresholds[i] for i in range(o.n_prim)]
         cands = [{"fp32_threshold": f, "prim_threshold": p, "ms": r.ms[k], "energy_error": r.energy_error[k]}
                  for k, (f, p) in enumerate((f, p) for f in fl for p in pl)]
+        k0 = len(cands)
+        for i in range(r.evaluated - k0):
+            cands.append({"tile": o.tiles[i], "ms": r.ms[k0 + i], "energy_error": r.energy_error[k0 + i]})
         best = JKOptions()
         ctypes.memmove(ctypes.byref(best), ctypes.byref(r.best), ctypes.sizeof(JKOptions))
         return best, {"found": bool(r.found), "best_ms": r.best_ms, "best_energy_error": r.best_energy_error,

@@ -64,12 +64,16 @@ typedef struct {
                                arrival order (default) */
   double mixed_threshold;   /* HFG_MIXED: quartets with Q_ab*Q_cd below this are
                                evaluated in FP32 and accumulated in FP64 */
+  int tile;                 /* quartet tile of the work queue: a warp takes up to
+                               `tile` tasks of 32 shell quartets per step, and
+                               steps are sized for tile/8 tasks of average cost
+                               per resident warp (0: 64) */
 } hfg_jk_opts;
 
 typedef struct hfg_ctx hfg_ctx;
 
 /* Default options: Schwarz 1e-12, no primitive screening, FP64, atomic
-   (not deterministic) accumulation. */
+   (not deterministic) accumulation, tile 64. */
 void hfg_jk_opts_default(hfg_jk_opts* opts);
 
 /*
@@ -203,8 +207,11 @@ int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* stats);
  * w = 1/4 for RHF (nspin 1) and 1/2 for UHF.  The fastest candidate with
  * |dE| <= max_energy_error is returned in `best` (schwarz_threshold from
  * `base`); if none qualifies, `best` is the FP64 options of `base` and
- * `found` is 0.  Empty candidate lists use 1e-9, 1e-8, 1e-7, 1e-6 (FP32) and
- * 1e-15, 1e-14, 1e-13 (primitives); the default budget is 5e-9 Eh.
+ * `found` is 0.  Then the best pair is timed with each quartet tile of
+ * `tiles` (hfg_jk_opts.tile) and the fastest within the budget kept.  Empty
+ * candidate lists use 1e-9, 1e-8, 1e-7, 1e-6 (FP32), 1e-15, 1e-14, 1e-13
+ * (primitives) and tiles 16, 256 (beside the default 64); the default budget
+ * is 5e-9 Eh.
  */
 typedef struct {
   double fp32_thresholds[8];
@@ -213,6 +220,8 @@ typedef struct {
   int n_prim;
   double max_energy_error;
   int repeats;
+  int tiles[4]; /* quartet tiles tried on the best threshold pair (hfg_jk_opts.tile) */
+  int n_tile;
 } hfg_autotune_opts;
 typedef struct {
   hfg_jk_opts best;
@@ -220,7 +229,8 @@ typedef struct {
   double best_ms, best_energy_error;
   double fp64_ms;                   /* the plain FP64 build */
   int evaluated;
-  double ms[64], energy_error[64];  /* per candidate, FP32-threshold-major order */
+  double ms[64], energy_error[64];  /* per candidate: FP32-threshold-major order,
+                                       then one per tile on the best pair */
 } hfg_autotune_result;
 void hfg_autotune_opts_default(hfg_autotune_opts* opts);
 int hfg_jk_autotune(hfg_ctx* ctx, const hfg_jk_opts* base, int nspin, const double* d_P_total,
