@@ -420,18 +420,20 @@ def run_ours(args):
     t_step = tot_mixed / args.steps / 1000.0
     pipe_frac = (stats_mixed["wmd_flops_fp64"] / (p64 * 1e12) + stats_mixed["wmd_flops_fp32"] / (p32 * 1e12)) / t_step
     pipe_frac /= world  # against the pipes of all N GPUs
-    # DRAM bytes of one mixed build from the committed ncu summary (captured
-    # on (H2O)32; dominated by register spills of the L >= 4 classes)
+    # DRAM bytes of one mixed build of (H2O)64 from the committed ncu summary
+    # (dominated by register spills of the L >= 5 classes); other sizes
+    # have no capture
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "jk_kernel_1000_h2o32.md")
-    if os.path.exists(prof):
+    prof = os.path.join(ROOT, "profiles", "jk_dram_h2o64_mixed.md")
+    if os.path.exists(prof) and args.waters == 64:
         for ln in open(prof):
-            if ln.startswith("traffic_bytes_per_mixed_build_h2o32:"):
+            if ln.startswith("traffic_bytes_per_mixed_build_h2o64:"):
                 traffic = float(ln.split(":")[1])
     roofline = {"bound": "fp64", "achieved": pipe_frac * p64, "peak": p64, "unit": "TFLOP/s", "frac": pipe_frac,
                 "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read+write of one autotuned mixed build of (H2O)32 (the "
-                                  "full-size capture is not made); mostly register spills of the L>=4 classes",
+                "traffic_source": "ncu dram__bytes_read+write summed over the 42 launches of one mixed build "
+                                  "of (H2O)64 (profiles/jk_dram_h2o64_mixed.md); mostly register spills of the "
+                                  "L>=5 classes",
                 "peak_source": "measured FMA chains on this device (hfg_fma_peak); FP32 work weighted by the "
                                "measured FP32 peak %.1f TFLOP/s" % p32,
                 "work_unit": "McMurchie-Davidson flops per evaluated primitive quartet (hf-rs loops), "

@@ -1264,6 +1264,67 @@ int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, c
 
 extern "C" {
 
+int hfg_eri_gradient(hfg_ctx* ctx, double schwarz_threshold, int nspin, const double* P_total, const double* P_spin,
+                     int natom, double* grad) {
+  if (!ctx) return HFG_ERR_INVALID_INPUT;
+  if (!P_total || !P_spin || !grad) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  if (nspin < 1 || nspin > 2) return set_error(ctx, HFG_ERR_INVALID_INPUT, "nspin must be 1 or 2");
+  if (!(schwarz_threshold >= 0.0)) return set_error(ctx, HFG_ERR_INVALID_INPUT, "Schwarz threshold must be >= 0");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  AllocScope alloc_scope(ctx->stream);
+  cudaSetDevice(ctx->device);
+  // the derivative integrals raise one shell by one: shells up to d
+  if (ctx->lmax > kLMax)
+    return set_error(ctx, HFG_ERR_UNSUPPORTED, "ERI derivatives cover s, p and d shells");
+  std::vector<int> ao_atom(ctx->n);
+  for (const Shell& sh : ctx->shells) {
+    if (sh.atom < 0 || sh.atom >= natom)
+      return set_error(ctx, HFG_ERR_INVALID_INPUT, "natom must exceed every basis function's atom index");
+    for (int k = 0; k < ncart(sh.l); ++k) ao_atom[sh.ao + k] = sh.atom;
+  }
+  Plan* plan = nullptr;
+  int rc = build_plan(ctx, schwarz_threshold, 0.0, 0.0, HFG_FP64, 0, plan);
+  if (rc != HFG_OK) return rc;
+  const size_t nn = (size_t)ctx->n * ctx->n;
+  HFG_CUDA(ctx, ctx->d_D.alloc(nn));
+  HFG_CUDA(ctx, ctx->d_Ds.alloc(2 * nn));
+  HFG_CUDA(ctx, ctx->d_counters.alloc(plan->launches.size() + 1));
+  DevBuf<int> d_atom;
+  DevBuf<double> d_grad;
+  HFG_CUDA(ctx, d_atom.alloc(ctx->n));
+  HFG_CUDA(ctx, d_grad.alloc((size_t)3 * natom));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_D.p, P_total, nn * 8, cudaMemcpyHostToDevice, ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_Ds.p, P_spin, nspin * nn * 8, cudaMemcpyHostToDevice, ctx->stream));
+  HFG_CUDA(ctx, cudaMemcpyAsync(d_atom.p, ao_atom.data(), ctx->n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  HFG_CUDA(ctx, cudaMemsetAsync(d_grad.p, 0, (size_t)3 * natom * sizeof(double), ctx->stream));
+  HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.p, 0, (plan->launches.size() + 1) * 8, ctx->stream));
+  JKLaunchArgs a{};
+  a.pairs = ctx->d_pairs.p;
+  a.pairQ = ctx->d_pairQ.p;
+  a.thr = schwarz_threshold;
+  a.rec64 = ctx->d_rec64.p;
+  a.boys64 = ctx->d_boys64.p;
+  a.expt64 = ctx->d_expt64.p;
+  a.Dtot = ctx->d_D.p;
+  a.Dspin = ctx->d_Ds.p;
+  a.n = ctx->n;
+  a.nspin = nspin;
+  for (size_t l = 0; l < plan->launches.size(); ++l) {
+    const Launch& L = plan->launches[l];
+    a.counter = ctx->d_counters.p + l;
+    a.entries = L.d_entries;
+    a.prefix = L.d_prefix;
+    a.chunk_entry = L.d_chunk;
+    a.chunk_start = L.d_cstart;
+    a.nchunks = L.nchunks;
+    HFG_CUDA(ctx, launch_grad_md(L.la, L.lb, L.lc, L.ld, a, d_atom.p, d_grad.p, ctx->stream));
+  }
+  HFG_CUDA(ctx, cudaMemcpyAsync(grad, d_grad.p, (size_t)3 * natom * sizeof(double), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return HFG_OK;
+}
+
 // Packed tensor on the device: every quartet of the FP64 plan without
 // primitive screening (the plan holds each unique significant shell quartet
 // once), stored by eri_packed_kernel.

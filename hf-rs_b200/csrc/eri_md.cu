@@ -211,6 +211,40 @@ struct MDPrim {
   double p, inv_p, kp, PA[3];
 };
 
+// R_{tuv} = R^{0}_{tuv} for t+u+v <= L into R0, from S[0..2] = P - Q,
+// S[3] = -2 alpha and F[n] = F_n: level n from level n + 1 for n = L .. 0
+// (level n in R0 for even n, R1 for odd n), the block synchronised after
+// each level.
+__device__ void md_build_R(int L, double* R0, double* R1, const double* S, const double* F) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int n = L; n >= 0; --n) {
+    double* cur = (n & 1) ? R1 : R0;
+    const double* prev = (n & 1) ? R0 : R1;
+    const int m = L - n, e1 = m + 1, cube = e1 * e1 * e1;
+    for (int x = tid; x < cube; x += nt) {
+      const int t = x / (e1 * e1), u = (x / e1) % e1, v = x % e1;
+      if (t + u + v > m) continue;
+      double r;
+      if (t > 0) {
+        r = S[0] * prev[ridx(t - 1, u, v)];
+        if (t > 1) r += (t - 1) * prev[ridx(t - 2, u, v)];
+      } else if (u > 0) {
+        r = S[1] * prev[ridx(t, u - 1, v)];
+        if (u > 1) r += (u - 1) * prev[ridx(t, u - 2, v)];
+      } else if (v > 0) {
+        r = S[2] * prev[ridx(t, u, v - 1)];
+        if (v > 1) r += (v - 1) * prev[ridx(t, u, v - 2)];
+      } else {
+        double w = 1.0;
+        for (int k = 0; k < n; ++k) w *= S[3];
+        r = w * F[n];
+      }
+      cur[ridx(t, u, v)] = r;
+    }
+    __syncthreads();
+  }
+}
+
 // Adds one primitive quartet into s.out (every thread of the block takes
 // part; the caller synchronises before reusing the tables).
 __device__ void md_prim_quartet(const MDClass& c, const MDLayout& L, const MDShared& s, const MDPrim& P,
@@ -236,33 +270,7 @@ __device__ void md_prim_quartet(const MDClass& c, const MDLayout& L, const MDSha
     md_hermite_axis(s.Ek, ax, c.lc, c.ld, Q.PA[ax], Q.PA[ax] + CD[ax], 0.5 * Q.inv_p);
   }
   __syncthreads();
-  // R^{n} for n = L .. 0 (level n in R0 for even n, R1 for odd n)
-  for (int n = c.L; n >= 0; --n) {
-    double* cur = (n & 1) ? s.R1 : s.R0;
-    const double* prev = (n & 1) ? s.R0 : s.R1;
-    const int m = c.L - n, e1 = m + 1, cube = e1 * e1 * e1;
-    for (int x = tid; x < cube; x += nt) {
-      const int t = x / (e1 * e1), u = (x / e1) % e1, v = x % e1;
-      if (t + u + v > m) continue;
-      double r;
-      if (t > 0) {
-        r = s.S[0] * prev[ridx(t - 1, u, v)];
-        if (t > 1) r += (t - 1) * prev[ridx(t - 2, u, v)];
-      } else if (u > 0) {
-        r = s.S[1] * prev[ridx(t, u - 1, v)];
-        if (u > 1) r += (u - 1) * prev[ridx(t, u - 2, v)];
-      } else if (v > 0) {
-        r = s.S[2] * prev[ridx(t, u, v - 1)];
-        if (v > 1) r += (v - 1) * prev[ridx(t, u, v - 2)];
-      } else {
-        double w = 1.0;
-        for (int k = 0; k < n; ++k) w *= s.S[3];
-        r = w * s.F[n];
-      }
-      cur[ridx(t, u, v)] = r;
-    }
-    __syncthreads();
-  }
+  md_build_R(c.L, s.R0, s.R1, s.S, s.F);
   // G[ab][h] = sum_tuv E^{ab}_{tuv} R_{t+tau, u+nu, v+phi}
   for (int x = tid; x < L.nab * L.nherm; x += nt) {
     const int ab = x / L.nherm, h = x % L.nherm;
@@ -567,6 +575,291 @@ __global__ void __launch_bounds__(kMDThreads) jk_md_kernel(MDClass c, const JKLa
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Nuclear derivatives of the two-electron energy (the ERI part of the HF
+// gradient, hf-rs's contract_eri_derivatives, src/gradient.rs:33-69 with the
+// densities of :287-301).  With G = P_ab P_cd - x (P_ac P_bd + P_ad P_bc)
+// (x = 1/4 for a closed shell; per spin, x = 1/2 on the spin densities)
+// the energy is E2 = 1/2 sum_abcd (ab|cd) G_abcd, so over unique quartets
+//   dE2/dX = 4 sum w (d(ab|cd)/dX) G_abcd,
+// w the degeneracy weight of the J/K kernels.  A centre derivative of a
+// Gaussian raises and lowers its power, d/dA_x phi_a = 2 alpha phi_{a+1x}
+// - a_x phi_{a-1x}, so the derivative integrals use the same R table (one
+// order higher) with Hermite coefficients 2 alpha E^{i+1,j} - i E^{i-1,j};
+// the fourth centre follows from translational invariance.  Per primitive
+// quartet, G is first contracted with one side's Hermite coefficients and
+// R (W, V for the bra; X, U for the ket), then with the derivative
+// coefficients of the other side.
+struct GradArgs {
+  const JKEntry* entries;
+  const long long* prefix;
+  const long long* chunk_start;
+  const int* chunk_entry;
+  long long nchunks;
+  unsigned long long* counter;
+  const PairInfo* pairs;
+  const double* pairQ;
+  double thr;
+  const PrimRec64* rec;
+  const double* boys;
+  const double* expt;
+  const double* P;   // total density, n x n
+  const double* Ps;  // nspin spin densities
+  int nspin, n;
+  const int* ao_atom;
+  double* grad;  // natom x 3
+};
+
+struct GradLayout {
+  int nab, ncd, hab, hcd, hab1, hcd1;
+  int G, W, X, V, U, R0, R1, Eb, Ek, F, S, red, dbl_end;
+  __host__ __device__ GradLayout(const MDClass& c) {
+    nab = c.na * c.nb;
+    ncd = c.nc * c.nd;
+    hab = (c.lab + 1) * (c.lab + 2) * (c.lab + 3) / 6;
+    hcd = (c.lcd + 1) * (c.lcd + 2) * (c.lcd + 3) / 6;
+    hab1 = (c.lab + 2) * (c.lab + 3) * (c.lab + 4) / 6;
+    hcd1 = (c.lcd + 2) * (c.lcd + 3) * (c.lcd + 4) / 6;
+    G = 0;
+    W = G + nab * ncd;
+    X = W + nab * hcd;
+    V = X + ncd * hab;
+    U = V + nab * hab1;
+    R0 = U + ncd * hcd1;
+    R1 = R0 + kMDRCube;
+    Eb = R1 + kMDRCube;
+    Ek = Eb + 3 * kMDEAxis;
+    F = Ek + 3 * kMDEAxis;
+    S = F + 4 * kMDLMax + 8;
+    red = S + 16;
+    dbl_end = red + 9 * (kMDThreads / 32);
+  }
+  __host__ __device__ size_t bytes() const {
+    return (size_t)dbl_end * 8 + (size_t)(kMDHCube + 3 * kMDHCube + 4 * 10 * 3) * 4;
+  }
+};
+
+__global__ void __launch_bounds__(kMDThreads) grad_md_kernel(MDClass c, const GradArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const GradLayout L(c);
+  double* d = reinterpret_cast<double*>(smem_raw);
+  double *Gm = d + L.G, *W = d + L.W, *X = d + L.X, *V = d + L.V, *U = d + L.U;
+  double *R0 = d + L.R0, *R1 = d + L.R1, *Eb = d + L.Eb, *Ek = d + L.Ek, *F = d + L.F, *S = d + L.S;
+  double* red = d + L.red;
+  int* ip = reinterpret_cast<int*>(d + L.dbl_end);
+  int *hidx = ip, *hlist = ip + kMDHCube, *comp = ip + 4 * kMDHCube;
+  __shared__ long long s_step;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  // components of the four shells, and the Hermite triples in order of
+  // total degree (those of degree <= k are the first nherm(k))
+  {
+    const int ls[4] = {c.la, c.lb, c.lc, c.ld};
+    for (int x = tid; x < 4 * 10; x += nt) {
+      const int sh = x / 10, k = x % 10;
+      if (k < ncart(ls[sh])) md_component(ls[sh], k, comp + x * 3);
+    }
+    if (tid == 0) {
+      for (int x = 0; x < kMDHCube; ++x) hidx[x] = -1;
+      int h = 0;
+      for (int deg = 0; deg < kMDE; ++deg)
+        for (int t = deg; t >= 0; --t)
+          for (int u = deg - t; u >= 0; --u) {
+            const int v = deg - t - u;
+            hidx[(t * kMDE + u) * kMDE + v] = h;
+            hlist[3 * h] = t;
+            hlist[3 * h + 1] = u;
+            hlist[3 * h + 2] = v;
+            ++h;
+          }
+    }
+  }
+  const int n = a.n, NS = a.nspin;
+  const double xk = NS == 1 ? 0.25 : 0.5;
+  const int Lg = c.L + 1;
+  const int* ca = comp;
+  const int* cb = comp + 30;
+  const int* cc = comp + 60;
+  const int* cdd = comp + 90;
+  auto hm = [&](int t, int u, int v) { return hidx[(t * kMDE + u) * kMDE + v]; };
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_step = (long long)atomicAdd(a.counter, 1ull);
+    __syncthreads();
+    const long long step = s_step;
+    if (step >= a.nchunks) break;
+    const long long t0 = a.chunk_start[step], t1 = a.chunk_start[step + 1];
+    int e = a.chunk_entry[step];
+    for (long long w = t0; w < t1; ++w) {
+      while (a.prefix[e + 1] <= w) ++e;
+      const JKEntry ent = a.entries[e];
+      const int k0 = ent.k_lo + (int)(w - a.prefix[e]) * 32, k1 = min(k0 + 32, ent.k_hi);
+      const PairInfo bra = a.pairs[ent.bra];
+      for (int kidx = k0; kidx < k1; ++kidx) {
+        if (!(a.pairQ[kidx] * a.pairQ[ent.bra] > a.thr)) continue;
+        const PairInfo ket = a.pairs[kidx];
+        const int i0 = bra.ao_a, j0 = bra.ao_b, kk0 = ket.ao_a, l0 = ket.ao_b;
+        // G with the component scales of the four functions
+        for (int x = tid; x < L.nab * L.ncd; x += nt) {
+          const int ab = x / L.ncd, cd = x % L.ncd;
+          const int I = i0 + ab / c.nb, J = j0 + ab % c.nb, K = kk0 + cd / c.nd, M = l0 + cd % c.nd;
+          double g = a.P[(size_t)I * n + J] * a.P[(size_t)K * n + M];
+          for (int sp = 0; sp < NS; ++sp) {
+            const double* D = a.Ps + (size_t)sp * n * n;
+            g -= xk * (D[(size_t)I * n + K] * D[(size_t)J * n + M] + D[(size_t)I * n + M] * D[(size_t)J * n + K]);
+          }
+          Gm[x] = g * md_comp_scale(ca + (ab / c.nb) * 3) * md_comp_scale(cb + (ab % c.nb) * 3) *
+                  md_comp_scale(cc + (cd / c.nd) * 3) * md_comp_scale(cdd + (cd % c.nd) * 3);
+        }
+        double acc[9];
+        for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+        const double AB[3] = {bra.ABx, bra.ABy, bra.ABz}, CD[3] = {ket.ABx, ket.ABy, ket.ABz};
+        const double AC[3] = {bra.Ax - ket.Ax, bra.Ay - ket.Ay, bra.Az - ket.Az};
+        for (int ib = 0; ib < bra.npp; ++ib) {
+          const PrimRec64 rb = a.rec[bra.rec_off + (size_t)ib * bra.rec_stride];
+          for (int ik = 0; ik < ket.npp; ++ik) {
+            const PrimRec64 rk = a.rec[ket.rec_off + (size_t)ik * ket.rec_stride];
+            __syncthreads();  // G written; tables of the previous primitive quartet read
+            const MDPrim Pp = md_from_rec(rb, bra), Qp = md_from_rec(rk, ket);
+            if (tid == 0) {
+              double PQ[3];
+              for (int k = 0; k < 3; ++k) PQ[k] = AC[k] + Pp.PA[k] - Qp.PA[k];
+              const double sum = Pp.p + Qp.p, alpha = Pp.p * Qp.p / sum;
+              md_boys(alpha * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]), Lg, a.boys, a.expt, F);
+              S[0] = PQ[0];
+              S[1] = PQ[1];
+              S[2] = PQ[2];
+              S[3] = -2.0 * alpha;
+              S[4] = kTwoPiPow25 * Pp.kp * Qp.kp * rsqrt(sum);
+            } else if (tid >= 32 && tid < 35) {
+              const int ax = tid - 32;
+              md_hermite_axis(Eb, ax, c.la + 1, c.lb + 1, Pp.PA[ax], Pp.PA[ax] + AB[ax], 0.5 * Pp.inv_p);
+            } else if (tid >= 64 && tid < 67) {
+              const int ax = tid - 64;
+              md_hermite_axis(Ek, ax, c.lc + 1, c.ld + 1, Qp.PA[ax], Qp.PA[ax] + CD[ax], 0.5 * Qp.inv_p);
+            }
+            __syncthreads();
+            md_build_R(Lg, R0, R1, S, F);
+            // W[ab][h] = sum_cd G s(h) E^{cd}_h;  X[cd][h] = sum_ab G E^{ab}_h
+            for (int x = tid; x < L.nab * L.hcd + L.ncd * L.hab; x += nt) {
+              if (x < L.nab * L.hcd) {
+                const int ab = x / L.hcd, h = x % L.hcd;
+                const int ht = hlist[3 * h], hu = hlist[3 * h + 1], hv = hlist[3 * h + 2];
+                double v = 0.0;
+                for (int cd = 0; cd < L.ncd; ++cd) {
+                  const int* ec = cc + (cd / c.nd) * 3;
+                  const int* ed = cdd + (cd % c.nd) * 3;
+                  v += Gm[(size_t)ab * L.ncd + cd] * Ek[eidx(0, ec[0], ed[0], ht)] * Ek[eidx(1, ec[1], ed[1], hu)] *
+                       Ek[eidx(2, ec[2], ed[2], hv)];
+                }
+                W[x] = ((ht + hu + hv) & 1) ? -v : v;
+              } else {
+                const int y = x - L.nab * L.hcd, cd = y / L.hab, h = y % L.hab;
+                const int ht = hlist[3 * h], hu = hlist[3 * h + 1], hv = hlist[3 * h + 2];
+                double v = 0.0;
+                for (int ab = 0; ab < L.nab; ++ab) {
+                  const int* ea = ca + (ab / c.nb) * 3;
+                  const int* eb = cb + (ab % c.nb) * 3;
+                  v += Gm[(size_t)ab * L.ncd + cd] * Eb[eidx(0, ea[0], eb[0], ht)] * Eb[eidx(1, ea[1], eb[1], hu)] *
+                       Eb[eidx(2, ea[2], eb[2], hv)];
+                }
+                X[y] = v;
+              }
+            }
+            __syncthreads();
+            // V[ab][h'] = sum_h W[ab][h] R_{h'+h} (h' of degree <= lab + 1);
+            // U[cd][h'] = sum_h X[cd][h] R_{h+h'} (h' of degree <= lcd + 1)
+            for (int x = tid; x < L.nab * L.hab1 + L.ncd * L.hcd1; x += nt) {
+              if (x < L.nab * L.hab1) {
+                const int ab = x / L.hab1, h1 = x % L.hab1;
+                const int t = hlist[3 * h1], u = hlist[3 * h1 + 1], v = hlist[3 * h1 + 2];
+                double r = 0.0;
+                for (int h = 0; h < L.hcd; ++h)
+                  r += W[(size_t)ab * L.hcd + h] * R0[ridx(t + hlist[3 * h], u + hlist[3 * h + 1], v + hlist[3 * h + 2])];
+                V[x] = r;
+              } else {
+                const int y = x - L.nab * L.hab1, cd = y / L.hcd1, h1 = y % L.hcd1;
+                const int t = hlist[3 * h1], u = hlist[3 * h1 + 1], v = hlist[3 * h1 + 2];
+                double r = 0.0;
+                for (int h = 0; h < L.hab; ++h)
+                  r += X[(size_t)cd * L.hab + h] * R0[ridx(hlist[3 * h] + t, hlist[3 * h + 1] + u, hlist[3 * h + 2] + v)];
+                U[y] = ((t + u + v) & 1) ? -r : r;
+              }
+            }
+            __syncthreads();
+            // derivative coefficients against V (centres A, B) and U (C)
+            const double pref = S[4];
+            const double beta = rb.bp * rb.p, alpha_a = rb.p - beta;
+            const double delta = rk.bp * rk.p, gamma_c = rk.p - delta;
+            for (int x = tid; x < L.nab + L.ncd; x += nt) {
+              const bool braside = x < L.nab;
+              const int id = braside ? x : x - L.nab;
+              const int* e1 = braside ? ca + (id / c.nb) * 3 : cc + (id / c.nd) * 3;
+              const int* e2 = braside ? cb + (id % c.nb) * 3 : cdd + (id % c.nd) * 3;
+              const double* E = braside ? Eb : Ek;
+              const double* T = braside ? V + (size_t)id * L.hab1 : U + (size_t)id * L.hcd1;
+              // first centre (A or C), then second (B), each x, y, z
+              for (int centre = 0; centre < (braside ? 2 : 1); ++centre) {
+                const double ex = centre == 0 ? (braside ? alpha_a : gamma_c) : beta;
+                for (int ax = 0; ax < 3; ++ax) {
+                  int p0[3] = {e1[0], e1[1], e1[2]}, q0[3] = {e2[0], e2[1], e2[2]};
+                  int* dv = centre == 0 ? p0 : q0;  // the differentiated function's powers
+                  const int lo = dv[ax];
+                  double sacc = 0.0;
+                  // 2 ex (raised) - lo (lowered), each a product of three axes
+                  for (int term = 0; term < 2; ++term) {
+                    if (term == 1 && lo == 0) break;
+                    const double f = term == 0 ? 2.0 * ex : -(double)lo;
+                    dv[ax] = term == 0 ? lo + 1 : lo - 1;
+                    double s3 = 0.0;
+                    for (int t = 0; t <= p0[0] + q0[0]; ++t) {
+                      const double e0 = E[eidx(0, p0[0], q0[0], t)];
+                      for (int u = 0; u <= p0[1] + q0[1]; ++u) {
+                        const double e01 = e0 * E[eidx(1, p0[1], q0[1], u)];
+                        for (int v = 0; v <= p0[2] + q0[2]; ++v)
+                          s3 += e01 * E[eidx(2, p0[2], q0[2], v)] * T[hm(t, u, v)];
+                      }
+                    }
+                    sacc += f * s3;
+                    dv[ax] = lo;
+                  }
+                  acc[(braside ? 3 * centre : 6) + ax] += pref * sacc;
+                }
+              }
+            }
+          }
+        }
+        // block sums of the nine components, then the four centres
+        for (int k = 0; k < 9; ++k) {
+          double v = acc[k];
+          for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+          if ((tid & 31) == 0) red[k * (kMDThreads / 32) + (tid >> 5)] = v;
+        }
+        __syncthreads();
+        if (tid == 0) {
+          double g[9];
+          for (int k = 0; k < 9; ++k) {
+            g[k] = 0.0;
+            for (int wv = 0; wv < nt / 32; ++wv) g[k] += red[k * (kMDThreads / 32) + wv];
+          }
+          double deg = 1.0;
+          if (bra.same) deg *= 0.5;
+          if (ket.same) deg *= 0.5;
+          if (kidx == ent.bra) deg *= 0.5;
+          const double f = 4.0 * deg;
+          const int atA = a.ao_atom[i0], atB = a.ao_atom[j0], atC = a.ao_atom[kk0], atD = a.ao_atom[l0];
+          for (int ax = 0; ax < 3; ++ax) {
+            atomicAdd(a.grad + 3 * atA + ax, f * g[ax]);
+            atomicAdd(a.grad + 3 * atB + ax, f * g[3 + ax]);
+            atomicAdd(a.grad + 3 * atC + ax, f * g[6 + ax]);
+            atomicAdd(a.grad + 3 * atD + ax, -f * (g[ax] + g[3 + ax] + g[6 + ax]));
+          }
+        }
+      }
+    }
+  }
+}
+
 int md_resident_blocks(const void* kern, size_t smem) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
@@ -645,6 +938,39 @@ cudaError_t launch_jk_md(int la, int lb, int lc, int ld, const JKLaunchArgs& a, 
   long long grid = a.serial ? 1 : md_resident_blocks((const void*)jk_md_kernel, smem);
   if (grid > a.nchunks) grid = a.nchunks;
   jk_md_kernel<<<(unsigned)grid, kMDThreads, smem, st>>>(c, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grad_md(int la, int lb, int lc, int ld, const JKLaunchArgs& j, const int* ao_atom, double* grad,
+                           cudaStream_t st) {
+  if (!md_class_ok(la, lb, lc, ld) || la > kMDLMax - 1 || lb > kMDLMax - 1 || lc > kMDLMax - 1 || ld > kMDLMax - 1)
+    return cudaErrorInvalidValue;
+  if (j.nchunks <= 0) return cudaSuccess;
+  const MDClass c = md_class(la, lb, lc, ld);
+  GradArgs a;
+  a.entries = j.entries;
+  a.prefix = j.prefix;
+  a.chunk_start = j.chunk_start;
+  a.chunk_entry = j.chunk_entry;
+  a.nchunks = j.nchunks;
+  a.counter = j.counter;
+  a.pairs = j.pairs;
+  a.pairQ = j.pairQ;
+  a.thr = j.thr;
+  a.rec = j.rec64;
+  a.boys = j.boys64;
+  a.expt = j.expt64;
+  a.P = j.Dtot;
+  a.Ps = j.Dspin;
+  a.nspin = j.nspin;
+  a.n = j.n;
+  a.ao_atom = ao_atom;
+  a.grad = grad;
+  const size_t smem = GradLayout(c).bytes();
+  cudaFuncSetAttribute(grad_md_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  long long grid = md_resident_blocks((const void*)grad_md_kernel, smem);
+  if (grid > j.nchunks) grid = j.nchunks;
+  grad_md_kernel<<<(unsigned)grid, kMDThreads, smem, st>>>(c, a);
   return cudaGetLastError();
 }
 

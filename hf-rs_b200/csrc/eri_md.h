@@ -30,5 +30,9 @@ cudaError_t launch_eri_packed_md(int la, int lb, int lc, int ld, const JKEntry* 
                                  const double* expt, double* out, cudaStream_t st);
 // FP64 J/K over the launch's work queue (a.serial: one block, deterministic)
 cudaError_t launch_jk_md(int la, int lb, int lc, int ld, const JKLaunchArgs& a, cudaStream_t st);
+// Nuclear derivatives of the two-electron energy over the launch's work
+// queue (densities a.Dtot, a.Dspin; shells up to d): adds into grad[atom][3]
+cudaError_t launch_grad_md(int la, int lb, int lc, int ld, const JKLaunchArgs& a, const int* ao_atom, double* grad,
+                           cudaStream_t st);
 
 }  // namespace hfg

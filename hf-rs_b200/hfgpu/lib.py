@@ -157,6 +157,7 @@ def load_library():
     L.hfg_jk_device_shard.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP, ctypes.c_int, ctypes.c_int]
     L.hfg_jk_device_noalloc.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
     L.hfg_jk_device_batch.argtypes = [P(VP), ctypes.c_int, P(JKOptions), P(VP), P(VP), P(VP), VP]
+    L.hfg_eri_gradient.argtypes = [VP, ctypes.c_double, ctypes.c_int, DP, DP, ctypes.c_int, DP]
     L.hfg_fock_rhf.argtypes = [VP, P(JKOptions), DP, DP, DP]
     L.hfg_fock_uhf.argtypes = [VP, P(JKOptions), DP, DP, DP, DP, DP]
     L.hfg_jk_last_stats.argtypes = [VP, P(JKStats)]
@@ -301,6 +302,18 @@ class Context:
         """Device-pointer form (integers); runs on the context stream."""
         o = opts or JKOptions.make()
         self._check(self.lib.hfg_jk_device(self.h, ctypes.byref(o), nspin, d_total, d_spin, d_J, d_K))
+
+    def eri_gradient(self, P_total, P_spin=None, schwarz=1e-12):
+        """Two-electron part of the nuclear gradient (hfg_eri_gradient):
+        (natom, 3) array of dE2/dR for the context's basis; P_spin None for
+        a closed shell, else the two spin densities."""
+        pt = np.ascontiguousarray(P_total, dtype=np.float64)
+        spins = [pt] if P_spin is None else list(P_spin)
+        ps = np.ascontiguousarray(np.stack(spins), dtype=np.float64)
+        natom = int(np.max(self.basis.atom)) + 1
+        g = np.zeros((natom, 3))
+        self._check(self.lib.hfg_eri_gradient(self.h, schwarz, len(spins), _dp(pt), _dp(ps), natom, _dp(g)))
+        return g
 
     @staticmethod
     def jk_device_batch(contexts, d_P, d_J, d_K, opts=None, stream=None):

@@ -175,6 +175,20 @@ int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, cons
 int hfg_jk_device_batch(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, const double* const* d_P,
                         double* const* d_J, double* const* d_K, void* stream);
 
+/*
+ * Stands in for contract_eri_derivatives with the RHF / UHF densities of
+ * compute_gradient_from_density (src/gradient.rs:33-69, :287-301) and the
+ * UHF driver: the two-electron part of the analytic nuclear gradient,
+ * grad[3 * atom + axis] = dE2/dR, E2 = 1/2 sum (ab|cd) (P_ab P_cd - x
+ * (P_ac P_bd + P_ad P_bc)) with x = 1/4 on P_total (nspin 1, P_spin =
+ * P_total) or x = 1/2 per spin density (nspin 2).  Host pointers; `natom`
+ * must exceed every basis function's atom index.  Shells up to d (the
+ * derivative integrals raise one shell to f); quartets with Q_ab Q_cd <=
+ * schwarz_threshold are skipped.
+ */
+int hfg_eri_gradient(hfg_ctx* ctx, double schwarz_threshold, int nspin, const double* P_total, const double* P_spin,
+                     int natom, double* grad);
+
 /* Stands in for build_fock_matrix (src/scf.rs:366-369): F = H + J - K/2. */
 int hfg_fock_rhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* P, double* F);
 

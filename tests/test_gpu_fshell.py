@@ -128,10 +128,13 @@ def test_scf_matches_oracle_energy(spdf, golden_dir, space):
 
 
 def test_f_shells_outside_the_generic_engine_are_rejected(spdf):
-    # density fitting and cross-molecule batches cover s, p and d
+    # density fitting covers orbital s, p and d shells
     ctx = Context(spdf["ours"])
     aux = CartesianBasis(spdf["atoms"], read_gaussian94(str(spdf["g"]["basis"])))
     from hfgpu.lib import DFTensor, HFG_DF_FP64
     with pytest.raises(HfgError, match="s, p and d"):
         DFTensor(ctx, aux, storage=HFG_DF_FP64)
+    # ERI derivatives raise a shell by one: f is beyond them
+    with pytest.raises(HfgError, match="s, p and d"):
+        ctx.eri_gradient(np.eye(ctx.n))
     ctx.close()
