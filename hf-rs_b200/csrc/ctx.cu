@@ -1325,6 +1325,40 @@ int hfg_eri_gradient(hfg_ctx* ctx, double schwarz_threshold, int nspin, const do
   return HFG_OK;
 }
 
+int hfg_gradient(hfg_ctx* ctx, int natom, const double* positions, const double* charges, int nspin,
+                 const double* P_total, const double* P_spin, const double* W, double schwarz_threshold,
+                 double* grad) {
+  if (!ctx) return HFG_ERR_INVALID_INPUT;
+  if (!positions || !charges || !P_total || !P_spin || !W || !grad)
+    return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
+  if (natom < 1 || natom > 4096) return set_error(ctx, HFG_ERR_INVALID_INPUT, "natom must be in 1..4096");
+  // two-electron part (its own lock and checks)
+  std::vector<double> g2(3 * (size_t)natom, 0.0);
+  int rc = hfg_eri_gradient(ctx, schwarz_threshold, nspin, P_total, P_spin, natom, g2.data());
+  if (rc != HFG_OK) return rc;
+  std::vector<double> g(3 * (size_t)natom, 0.0);
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    AllocScope alloc_scope(ctx->stream);
+    cudaSetDevice(ctx->device);
+    rc = one_electron_gradient(ctx, natom, positions, charges, P_total, W, g.data());
+    if (rc != HFG_OK) return rc;
+  }
+  // nuclear repulsion: -sum_B Z_A Z_B (R_A - R_B) / |R_A - R_B|^3
+  for (int A = 0; A < natom; ++A)
+    for (int B = 0; B < natom; ++B) {
+      if (A == B) continue;
+      const double d[3] = {positions[3 * A] - positions[3 * B], positions[3 * A + 1] - positions[3 * B + 1],
+                           positions[3 * A + 2] - positions[3 * B + 2]};
+      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      if (!(r2 > 0.0)) return set_error(ctx, HFG_ERR_INVALID_INPUT, "coincident nuclei");
+      const double f = -charges[A] * charges[B] / (r2 * std::sqrt(r2));
+      for (int k = 0; k < 3; ++k) g[3 * A + k] += f * d[k];
+    }
+  for (size_t x = 0; x < g.size(); ++x) grad[x] = g[x] + g2[x];
+  return HFG_OK;
+}
+
 // Packed tensor on the device: every quartet of the FP64 plan without
 // primitive screening (the plan holds each unique significant shell quartet
 // once), stored by eri_packed_kernel.

@@ -202,6 +202,11 @@ int batcher_submit(JKBatcher* b, hfg_ctx* ctx, const hfg_jk_opts& o, const doubl
 // n_p (n_p + 1) / 2), quartets with Q_ab Q_cd > thr; the context lock held.
 int eri_packed_locked(hfg_ctx* ctx, double thr, double* d_out, size_t len);
 int build_shell_list(hfg_ctx* ctx, const hfg_basis* b, int lmax);
+// Implemented in oneint.cu: the one-electron terms of the nuclear gradient
+// (basis derivatives of S, T, V against W and P, and the operator derivative
+// of V) added into grad (host, natom x 3); the context lock held.
+int one_electron_gradient(hfg_ctx* ctx, int natom, const double* pos, const double* charge, const double* P,
+                          const double* W, double* grad);
 void make_pair(const hfg_ctx* ctx, int a, int b, PairInfo& pi, std::vector<PrimPair>& pp, int owner);
 int cuda_check(hfg_ctx* ctx, cudaError_t e, const char* what);
 }  // namespace hfg

@@ -158,6 +158,7 @@ def load_library():
     L.hfg_jk_device_noalloc.argtypes = [VP, P(JKOptions), ctypes.c_int, VP, VP, VP, VP]
     L.hfg_jk_device_batch.argtypes = [P(VP), ctypes.c_int, P(JKOptions), P(VP), P(VP), P(VP), VP]
     L.hfg_eri_gradient.argtypes = [VP, ctypes.c_double, ctypes.c_int, DP, DP, ctypes.c_int, DP]
+    L.hfg_gradient.argtypes = [VP, ctypes.c_int, DP, DP, ctypes.c_int, DP, DP, DP, ctypes.c_double, DP]
     L.hfg_fock_rhf.argtypes = [VP, P(JKOptions), DP, DP, DP]
     L.hfg_fock_uhf.argtypes = [VP, P(JKOptions), DP, DP, DP, DP, DP]
     L.hfg_jk_last_stats.argtypes = [VP, P(JKStats)]
@@ -314,6 +315,41 @@ class Context:
         g = np.zeros((natom, 3))
         self._check(self.lib.hfg_eri_gradient(self.h, schwarz, len(spins), _dp(pt), _dp(ps), natom, _dp(g)))
         return g
+
+    def gradient(self, P_total, W, P_spin=None, schwarz=1e-12):
+        """Analytic nuclear gradient (hfg_gradient), (natom, 3) in hartree/bohr,
+        from the SCF's total density, energy-weighted density W and (open
+        shell) spin densities, all in the Cartesian basis."""
+        b = self.basis
+        pos = np.ascontiguousarray(b.positions())
+        chg = np.ascontiguousarray(b.nuclear_charges())
+        pt = np.ascontiguousarray(P_total, dtype=np.float64)
+        spins = [pt] if P_spin is None else list(P_spin)
+        ps = np.ascontiguousarray(np.stack(spins), dtype=np.float64)
+        w = np.ascontiguousarray(W, dtype=np.float64)
+        g = np.zeros((len(chg), 3))
+        self._check(self.lib.hfg_gradient(self.h, len(chg), _dp(pos), _dp(chg), len(spins), _dp(pt), _dp(ps), _dp(w),
+                                          schwarz, _dp(g)))
+        return g
+
+    def scf_gradient(self, charge=0, multiplicity=1, uhf=False, spherical=False, tol=1e-10, max_iter=100):
+        """SCF (hfg_scf) and its analytic gradient: returns (result dict,
+        (natom, 3) gradient).  W = sum over occupied orbitals of eps C C^T
+        per spin (x 2 for a closed shell)."""
+        r = self.scf(charge=charge, multiplicity=multiplicity, uhf=uhf, spherical=spherical, tol=tol,
+                     max_iter=max_iter, want=("P", "C", "eps"))
+        nel = int(round(float(np.sum(self.basis.nuclear_charges())))) - charge
+        if uhf:
+            na = (nel + multiplicity - 1) // 2
+            occ = [na, nel - na]
+            W = sum(r["C"][s][:, :occ[s]] @ np.diag(r["eps"][s][:occ[s]]) @ r["C"][s][:, :occ[s]].T for s in range(2))
+            g = self.gradient(r["P"][0] + r["P"][1], W, P_spin=[r["P"][0], r["P"][1]])
+        else:
+            no = nel // 2
+            C = r["C"][0][:, :no]
+            W = 2.0 * C @ np.diag(r["eps"][0][:no]) @ C.T
+            g = self.gradient(r["P"][0], W)
+        return r, g
 
     @staticmethod
     def jk_device_batch(contexts, d_P, d_J, d_K, opts=None, stream=None):

@@ -189,6 +189,21 @@ int hfg_jk_device_batch(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opt
 int hfg_eri_gradient(hfg_ctx* ctx, double schwarz_threshold, int nspin, const double* P_total, const double* P_spin,
                      int natom, double* grad);
 
+/*
+ * Stands in for compute_gradient_from_density (src/gradient.rs:287-455), as
+ * compute_rhf_gradient / compute_uhf_gradient call it: the analytic nuclear
+ * gradient dE/dR (grad[3 * atom + axis], hartree/bohr) of an SCF solution
+ * given its total density P_total, its spin densities as hfg_eri_gradient
+ * takes them, and the energy-weighted density W = sum_occ eps_i C_i C_i^T
+ * (x 2 for a closed shell), all host n x n in the Cartesian basis: nuclear
+ * repulsion, the one-electron terms (basis derivatives of S, T, V and the
+ * operator derivative of V) and the two-electron terms.  Nuclei as in
+ * hfg_scf_opts (bohr).  Shells up to d.
+ */
+int hfg_gradient(hfg_ctx* ctx, int natom, const double* positions, const double* charges, int nspin,
+                 const double* P_total, const double* P_spin, const double* W, double schwarz_threshold,
+                 double* grad);
+
 /* Stands in for build_fock_matrix (src/scf.rs:366-369): F = H + J - K/2. */
 int hfg_fock_rhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const double* P, double* F);
 

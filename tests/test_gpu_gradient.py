@@ -65,3 +65,32 @@ def test_eri_gradient_rejects_too_few_atoms():
     rc = ctx.lib.hfg_eri_gradient(ctx.h, 1e-12, 1, _dp(P), _dp(P), 1, _dp(g))
     assert rc != 0 and b"natom" in ctx.lib.hfg_last_error(ctx.h)
     ctx.close()
+
+
+def scf_energy(atoms, name, spherical, charge=0, multiplicity=1, uhf=False):
+    ctx = Context(CartesianBasis.build(atoms, name))
+    r = ctx.scf(charge=charge, multiplicity=multiplicity, uhf=uhf, spherical=spherical, tol=1e-11, want=())
+    ctx.close()
+    assert r["converged"]
+    return r["energy"]
+
+
+@pytest.mark.parametrize("name,nw,spherical,uhf", [("cc-pvdz", 1, True, False), ("6-31g*", 2, False, False),
+                                                   ("6-31g*", 1, False, True)])
+def test_full_gradient_matches_finite_differences_of_the_scf_energy(name, nw, spherical, uhf):
+    # hfg_gradient (nuclear repulsion + one-electron + two-electron terms) of
+    # a converged SCF against fourth-order central differences of the SCF
+    # energy itself: RHF in the spherical and Cartesian spaces, and the UHF
+    # doublet cation
+    atoms = water_cluster(nw)
+    charge, mult = (1, 2) if uhf else (0, 1)
+    ctx = Context(CartesianBasis.build(atoms, name))
+    r, g = ctx.scf_gradient(charge=charge, multiplicity=mult, uhf=uhf, spherical=spherical, tol=1e-11)
+    ctx.close()
+    assert r["converged"] and g.shape == (len(atoms), 3)
+    assert np.max(np.abs(g.sum(axis=0))) < 1e-8
+    h = 2e-3
+    for at, ax in ((0, 0), (0, 2), (1, 1), (len(atoms) - 1, 0)):
+        f = {k: scf_energy(shifted(atoms, at, ax, k * h), name, spherical, charge, mult, uhf) for k in (-2, -1, 1, 2)}
+        fd = (8.0 * (f[1] - f[-1]) - (f[2] - f[-2])) / (12.0 * h)
+        assert abs(fd - g[at, ax]) < 1e-6, (at, ax, fd, g[at, ax])
