@@ -50,8 +50,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--serve-jobs", type=int, default=24)
-    ap.add_argument("--serve-max-waters", type=int, default=16)
+    ap.add_argument("--serve-jobs", type=int, default=16)
+    ap.add_argument("--serve-max-waters", type=int, default=48)
     ap.add_argument("--df-waters", type=int, default=48, help="also time DF J/K on (H2O)_n (0: skip)")
     ap.add_argument("--scf-waters", type=int, default=-1,
                     help="full SCF in FP64 and in the mixed form on (H2O)_n (-1: --waters, 0: skip)")

@@ -29,6 +29,9 @@ static cudaError_t launch_t(const JKLaunchArgs& a, cudaStream_t st) {
   if (resident <= 0) {
     int sms = 0, per_sm = 0;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+#ifdef HFG_JK_CARVEOUT
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, HFG_JK_CARVEOUT);
+#endif
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem);
     resident = sms * (per_sm > 0 ? per_sm : 1);

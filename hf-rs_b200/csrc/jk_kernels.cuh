@@ -169,10 +169,13 @@ __device__ __forceinline__ void digest(const DT* __restrict__ w, const PairInfo&
 template <int LA, int LB, int LC, int LD, typename T> struct MinBlocks {
   static constexpr int code = LA * 1000 + LB * 100 + LC * 10 + LD;
   static constexpr int L = LA + LB + LC + LD;
+#ifndef HFG_JK_F64_LIGHT_BLOCKS
+#define HFG_JK_F64_LIGHT_BLOCKS 2
+#endif
 #ifdef HFG_JK_MIN_BLOCKS_F64
   static constexpr int f64 = HFG_JK_MIN_BLOCKS_F64;
 #else
-  static constexpr int f64 = L >= 4 ? 1 : 2;
+  static constexpr int f64 = L >= 4 ? 1 : (L <= 2 ? HFG_JK_F64_LIGHT_BLOCKS : 2);
 #endif
 #ifdef HFG_JK_MIN_BLOCKS_F32
   static constexpr int f32 = HFG_JK_MIN_BLOCKS_F32;
