@@ -347,6 +347,32 @@ static int build_pairs(hfg_ctx* ctx) {
   }
   HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_pairs.p, ctx->h_pairs.data(), ctx->h_pairs.size() * sizeof(PairInfo),
                                 cudaMemcpyHostToDevice, ctx->stream));
+  {
+    const size_t np2 = ctx->h_pairs.size();
+    std::vector<double2> a0(np2), a1(np2), a2(np2);
+    std::vector<int4> ii(np2);
+    std::vector<int2> nn(np2);
+    for (size_t k = 0; k < np2; ++k) {
+      const PairInfo& q = ctx->h_pairs[k];
+      a0[k] = make_double2(q.Ax, q.Ay);
+      a1[k] = make_double2(q.Az, q.ABx);
+      a2[k] = make_double2(q.ABy, q.ABz);
+      ii[k] = make_int4(q.ao_a, q.ao_b, q.rec_off, q.rec_stride);
+      nn[k] = make_int2(q.npp, q.same);
+    }
+    HFG_CUDA(ctx, ctx->d_ka0.alloc(np2));
+    HFG_CUDA(ctx, ctx->d_ka1.alloc(np2));
+    HFG_CUDA(ctx, ctx->d_ka2.alloc(np2));
+    HFG_CUDA(ctx, ctx->d_kii.alloc(np2));
+    HFG_CUDA(ctx, ctx->d_knn.alloc(np2));
+    HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_ka0.p, a0.data(), np2 * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+    HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_ka1.p, a1.data(), np2 * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+    HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_ka2.p, a2.data(), np2 * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+    HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_kii.p, ii.data(), np2 * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+    HFG_CUDA(ctx, cudaMemcpyAsync(ctx->d_knn.p, nn.data(), np2 * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+    // the host vectors go out of scope: the copies must have read them
+    HFG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   HFG_CUDA(ctx, ctx->d_rec64.alloc(npp));
   HFG_CUDA(ctx, ctx->d_rec32.alloc(npp));
   HFG_CUDA(ctx, ctx->d_pbound.alloc(npp));
@@ -684,6 +710,7 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   }
   JKLaunchArgs a{};
   a.pairs = ctx->d_pairs.p;
+  a.kets = ctx->kets();
   a.pairQ = ctx->d_pairQ.p;
   a.thr = o.schwarz_threshold;
   a.rec64 = ctx->d_rec64.p;
@@ -831,6 +858,11 @@ hfg_ctx::~hfg_ctx() {
   // destroyed (their frees are ordered on it)
   d_pairQ.release();
   d_pairs.release();
+  d_ka0.release();
+  d_ka1.release();
+  d_ka2.release();
+  d_kii.release();
+  d_knn.release();
   d_prims.release();
   d_rec64.release();
   d_rec32.release();
@@ -1189,6 +1221,7 @@ int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, c
       x.chunk_start = L.d_cstart;
       x.chunk_entry = L.d_chunk;
       x.pairs = c->d_pairs.p;
+      x.kets = c->kets();
       x.pairQ = c->d_pairQ.p;
       x.rec64 = c->d_rec64.p;
       x.rec32 = c->d_rec32.p;
@@ -1300,6 +1333,7 @@ int hfg_eri_gradient(hfg_ctx* ctx, double schwarz_threshold, int nspin, const do
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.p, 0, (plan->launches.size() + 1) * 8, ctx->stream));
   JKLaunchArgs a{};
   a.pairs = ctx->d_pairs.p;
+  a.kets = ctx->kets();
   a.pairQ = ctx->d_pairQ.p;
   a.thr = schwarz_threshold;
   a.rec64 = ctx->d_rec64.p;

@@ -153,6 +153,11 @@ struct hfg_ctx {
   std::vector<hfg::PairClass> classes;
 
   hfg::DevBuf<hfg::PairInfo> d_pairs;
+  // ket-side fields of d_pairs as separate arrays (hfg::KetSoA)
+  hfg::DevBuf<double2> d_ka0, d_ka1, d_ka2;
+  hfg::DevBuf<int4> d_kii;
+  hfg::DevBuf<int2> d_knn;
+  hfg::KetSoA kets() const { return hfg::KetSoA{d_ka0.p, d_ka1.p, d_ka2.p, d_kii.p, d_knn.p}; }
   hfg::DevBuf<hfg::PrimPair> d_prims;
   hfg::DevBuf<hfg::PrimRec64> d_rec64;
   hfg::DevBuf<hfg::PrimRec32> d_rec32;

@@ -44,6 +44,18 @@ struct __align__(16) PrimRec32 {
   float p, inv_p, kp, bp;
 };
 
+// The ket-side fields of the sorted pair table as separate arrays, so that
+// the 32 lanes of a warp, which hold consecutive kets, load each field
+// with coalesced 16-byte accesses (the 80-byte PairInfo records would
+// spread one field over 20 cache lines).
+struct KetSoA {
+  const double2* a0;  // Ax, Ay
+  const double2* a1;  // Az, ABx
+  const double2* a2;  // ABy, ABz
+  const int4* ii;     // ao_a, ao_b, rec_off, rec_stride
+  const int2* nn;     // npp, same
+};
+
 // Work entry of one J/K launch: bra pair and the range of ket pairs
 // [k_lo, k_hi) (global pair indices, kets of one pair class).
 struct JKEntry {
@@ -62,6 +74,7 @@ struct JKJob {
   const PrimRec64* rec64;
   const PrimRec32* rec32;
   const float* pbound;
+  KetSoA kets;
   const double* Dtot;
   double* Jacc;
   double* Kacc;
@@ -78,6 +91,7 @@ struct JKLaunchArgs {
   long long nchunks;
   long long nwarps;
   const PairInfo* pairs;
+  KetSoA kets;          // ket-side fields of `pairs` (same indexing)
   const double* pairQ;  // Schwarz bound per pair; a lane's quartet counts if Q_bra Q_ket > thr
   double thr;
   const PrimRec64* rec64;

@@ -249,12 +249,29 @@ __device__ __forceinline__ void jk_step(const JKLaunchArgs& a, long long c, int 
         const bool active = kidx < ent.k_hi && __ldg(a.pairQ + kidx) * __ldg(a.pairQ + ent.bra) > a.thr &&
                             (rounds == 1 || lane == round);
         const PairInfo bra = a.pairs[ent.bra];
-        const PairInfo ket = a.pairs[active ? kidx : ent.k_lo];
-        // the next task usually continues this entry: start fetching its ket
-        // pair, and its first primitive records (kets of one class have equal
-        // primitive counts and consecutive records, so they start 32 on)
+        PairInfo ket;
+        {
+          const int kx = active ? kidx : ent.k_lo;
+          const double2 v0 = __ldg(a.kets.a0 + kx), v1 = __ldg(a.kets.a1 + kx), v2 = __ldg(a.kets.a2 + kx);
+          const int4 ii = __ldg(a.kets.ii + kx);
+          const int2 nn = __ldg(a.kets.nn + kx);
+          ket.Ax = v0.x;
+          ket.Ay = v0.y;
+          ket.Az = v1.x;
+          ket.ABx = v1.y;
+          ket.ABy = v2.x;
+          ket.ABz = v2.y;
+          ket.ao_a = ii.x;
+          ket.ao_b = ii.y;
+          ket.rec_off = ii.z;
+          ket.rec_stride = ii.w;
+          ket.npp = nn.x;
+          ket.same = nn.y;
+        }
+        // the next task usually continues this entry: start fetching its
+        // first primitive records (kets of one class have equal primitive
+        // counts and consecutive records, so they start 32 on)
         if (HFG_JK_PREFETCH && warp + 1 < t1 && kidx + 32 < ent.k_hi) {
-          prefetch_l1(&a.pairs[kidx + 32]);
           prefetch_l1(RecOf<T>::get(a) + ket.rec_off + 32);
           prefetch_l1(a.pbound + ket.rec_off + 32);
         }
@@ -442,6 +459,7 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
     la.chunk_start = jb.chunk_start;
     la.chunk_entry = jb.chunk_entry;
     la.pairs = jb.pairs;
+    la.kets = jb.kets;
     la.pairQ = jb.pairQ;
     la.rec64 = jb.rec64;
     la.rec32 = jb.rec32;

@@ -112,6 +112,7 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
   if (rc != HFG_OK) return rc;
   hfg::JKLaunchArgs a{};
   a.pairs = ctx->d_pairs.p;
+  a.kets = ctx->kets();
   a.pairQ = ctx->d_pairQ.p;
   a.thr = o.schwarz_threshold;
   a.rec64 = ctx->d_rec64.p;
