@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(kMDThreads) eri_packed_md_kernel(
 // (jk_kernels.cuh): J'[a,b] += 4w sum D[c,d], J'[c,d] += 4w sum D[a,b],
 // K'[a,c] += 2w sum D[b,d] and the three other exchange blocks, w the
 // quartet's degeneracy weight.  In deterministic mode one block runs the
-// queue and each element's atomic is issued by one thread, quartet after
+// queue and one thread issues every atomic of a quartet, quartet after
 // quartet.
 __global__ void __launch_bounds__(kMDThreads) jk_md_kernel(MDClass c, const JKLaunchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -511,7 +511,12 @@ __global__ void __launch_bounds__(kMDThreads) jk_md_kernel(MDClass c, const JKLa
         // items: J'[ab], J'[cd], then per spin K'[ac], K'[bc], K'[ad], K'[bd]
         const int nK = na * nc + nb * nc + na * nd + nb * nd;
         const int items = L.nab + L.ncd + NS * nK;
-        for (int x = threadIdx.x; x < items; x += blockDim.x) {
+        // items can add into the same element (J'[ab] and J'[cd] of a pair
+        // with itself, K' blocks of a same-shell pair): in deterministic mode
+        // one thread takes every item in order
+        const int x0 = a.serial ? (threadIdx.x == 0 ? 0 : items) : threadIdx.x;
+        const int dx = a.serial ? 1 : blockDim.x;
+        for (int x = x0; x < items; x += dx) {
           if (x < L.nab) {
             double v = 0.0;
             for (int cd = 0; cd < L.ncd; ++cd)
