@@ -235,19 +235,19 @@ __device__ __forceinline__ void jk_step(const JKLaunchArgs& a, long long c, int 
     const long long t0 = __ldg(a.chunk_start + c), t1 = __ldg(a.chunk_start + c + 1);
     int e = __ldg(a.chunk_entry + c);
     long long next = __ldg(a.prefix + e + 1);
-    const int rounds = a.serial ? 32 : 1;
+    const int turns = a.serial ? 32 : 1;
     for (long long warp = t0; warp < t1; ++warp) {
       while (warp >= next) {
         ++e;
         next = a.prefix[e + 1];
       }
-      for (int round = 0; round < rounds; ++round) {
+      for (int turn = 0; turn < turns; ++turn) {
         const JKEntry ent = a.entries[e];
         const int kidx = ent.k_lo + (int)(warp - a.prefix[e]) * 32 + lane;
         // kets are bucketed by bound: the exact Schwarz test per quartet (in
-        // deterministic mode, only lane `round`'s quartet this round)
+        // deterministic mode, only lane `turn`'s quartet on this turn)
         const bool active = kidx < ent.k_hi && __ldg(a.pairQ + kidx) * __ldg(a.pairQ + ent.bra) > a.thr &&
-                            (rounds == 1 || lane == round);
+                            (turns == 1 || lane == turn);
         const PairInfo bra = a.pairs[ent.bra];
         PairInfo ket;
         {
