@@ -160,7 +160,7 @@ extern "C" int hfg_cholesky_eri(hfg_ctx* ctx, double threshold, size_t budget, h
   CK(df->colmn.alloc(np));
   CK(cudaMemcpyAsync(df->colmn.p, colmn.data(), np * sizeof(int2), cudaMemcpyHostToDevice, st));
   CK(cudaStreamSynchronize(st));
-  df->naux = df->rank = (int)rank;
+  df->naux = df->rank = df->rank_total = (int)rank;
   df->ncol = np;
   if (max_residual) *max_residual = maxres;
   if (n_pivots) *n_pivots = (int)rank;

@@ -675,8 +675,10 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   hfg_jk_opts o;
   if (opts) o = *opts; else hfg_jk_opts_default(&o);
   if (nspin < 1 || nspin > 2) return set_error(ctx, HFG_ERR_INVALID_INPUT, "nspin must be 1 or 2");
+  // (a NaN threshold would break the ordering of the plan map)
   if (!(o.schwarz_threshold >= 0.0) || !(o.prim_threshold >= 0.0) ||
-      (o.precision != HFG_FP64 && o.precision != HFG_MIXED) || o.tile < 0 || o.tile > 4096)
+      (o.precision != HFG_FP64 && o.precision != HFG_MIXED) ||
+      (o.precision == HFG_MIXED && !(o.mixed_threshold >= 0.0)) || o.tile < 0 || o.tile > 4096)
     return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid J/K options");
   // a context served with others hands its RHF builds to their batcher
   if (ctx->batcher && nspin == 1 && nshards == 1 && dPs == dPt && !o.deterministic)
@@ -1129,7 +1131,8 @@ int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, c
     if (ctxs[j]->device != c0->device) return fail(HFG_ERR_INVALID_INPUT, "the contexts of a batch must share one device");
     if (ctxs[j]->lmax > kLMax) return fail(HFG_ERR_UNSUPPORTED, "batched builds cover s, p and d shells");
     if (!(o.schwarz_threshold >= 0.0) || !(o.prim_threshold >= 0.0) ||
-        (o.precision != HFG_FP64 && o.precision != HFG_MIXED) || o.tile < 0 || o.tile > 4096)
+        (o.precision != HFG_FP64 && o.precision != HFG_MIXED) ||
+        (o.precision == HFG_MIXED && !(o.mixed_threshold >= 0.0)) || o.tile < 0 || o.tile > 4096)
       return fail(HFG_ERR_INVALID_INPUT, "invalid J/K options");
   }
   // per molecule: its plan (built once, cached on its context) and its

@@ -135,8 +135,14 @@ extern "C" {
 
 int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, double pair_threshold, int storage,
                  hfg_df** out) {
+  return hfg_df_build_shard(ctx, aux, metric_cutoff, pair_threshold, storage, 0, 1, out);
+}
+
+int hfg_df_build_shard(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, double pair_threshold, int storage,
+                       int shard, int nshards, hfg_df** out) {
   if (!ctx || !aux || !out) return HFG_ERR_INVALID_INPUT;
   *out = nullptr;
+  if (nshards < 1 || shard < 0 || shard >= nshards) return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid shard");
   if (!(metric_cutoff > 0) || !std::isfinite(metric_cutoff))
     return set_error(ctx, HFG_ERR_INVALID_INPUT, "DF metric cutoff must be finite and positive");
   if (storage < HFG_DF_FP64 || storage > HFG_DF_BF16) return set_error(ctx, HFG_ERR_INVALID_INPUT, "storage");
@@ -205,17 +211,24 @@ int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, doubl
   if (wh[0] < -metric_cutoff) return set_error(ctx, HFG_ERR_INTEGRAL, "DF metric has a negative eigenvalue");
   int first = 0;
   while (first < naux && wh[first] < metric_cutoff) ++first;
-  const int rank = naux - first;
-  if (rank <= 0) return set_error(ctx, HFG_ERR_INTEGRAL, "DF metric has zero retained rank");
+  const int rank_total = naux - first;
+  if (rank_total <= 0) return set_error(ctx, HFG_ERR_INTEGRAL, "DF metric has zero retained rank");
+  // this shard's rows of B: whitened functions [row0, row0 + rank)
+  const int row0 = (int)((long long)rank_total * shard / nshards);
+  const int rank = (int)((long long)rank_total * (shard + 1) / nshards) - row0;
+  if (rank <= 0) return set_error(ctx, HFG_ERR_INVALID_INPUT, "more DF shards than retained auxiliary functions");
   df->rank = rank;
-  // Xm = V[:, first:] diag(w^-1/2), column-major naux x rank
+  df->rank_total = rank_total;
+  df->row0 = row0;
+  // Xm = V[:, first + row0 : first + row0 + rank] diag(w^-1/2), column-major
+  // naux x rank (columns move left only, so none is overwritten before use)
   {
     std::vector<double> Vh((size_t)naux * naux);
     CK(cudaMemcpyAsync(Vh.data(), V.p, Vh.size() * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     for (int c = 0; c < rank; ++c) {
-      const double sc = 1.0 / std::sqrt(wh[first + c]);
-      for (int r = 0; r < naux; ++r) Vh[(size_t)c * naux + r] = Vh[(size_t)(first + c) * naux + r] * sc;
+      const double sc = 1.0 / std::sqrt(wh[first + row0 + c]);
+      for (int r = 0; r < naux; ++r) Vh[(size_t)c * naux + r] = Vh[(size_t)(first + row0 + c) * naux + r] * sc;
     }
     CK(cudaMemcpyAsync(V.p, Vh.data(), (size_t)naux * rank * 8, cudaMemcpyHostToDevice, st));
   }
@@ -433,6 +446,8 @@ int hfg_df_three_center(hfg_ctx* ctx, const hfg_basis* aux, double* out, size_t 
 }  // extern "C"
 
 namespace hfg {
+
+bool df_is_shard(const hfg_df* df) { return df->shard(); }
 
 // J and K from occupied coefficients on the device: dC column-major n x nocc
 // (leading dimension n), i.e. the first nocc columns of an SCF C matrix.

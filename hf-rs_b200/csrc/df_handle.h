@@ -12,6 +12,9 @@
 struct hfg_df {
   hfg_ctx* ctx = nullptr;
   int n = 0, naux = 0, rank = 0;
+  // a shard factor holds rows [row0, row0 + rank) of the full rank_total rows
+  int rank_total = 0, row0 = 0;
+  bool shard() const { return rank != rank_total; }
   long long ncol = 0;
   int storage = HFG_DF_FP64;
   hfg::DevBuf<double> B64;

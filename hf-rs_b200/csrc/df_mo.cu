@@ -162,6 +162,8 @@ extern "C" int hfg_df_mp2(hfg_df* df, const double* C, const double* eps, int m,
   if (!C || !eps || !energy || m <= 0) return set_error(ctx, HFG_ERR_INVALID_INPUT, "null pointer");
   if (n_frozen < 0 || n_frozen > n_occ || n_occ > m)
     return set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid RI-MP2 orbital partition");
+  // (ia|jb) sums over every auxiliary function before the energy expression
+  if (df->shard()) return set_error(ctx, HFG_ERR_INVALID_INPUT, "RI-MP2 needs the whole factor, not a shard of it");
   const int no = n_occ - n_frozen, nv = m - n_occ;
   *energy = 0.0;
   if (no == 0 || nv == 0) return HFG_OK;

@@ -182,6 +182,8 @@ namespace hfg {
 // all of them).
 int df_jk_device(hfg_df* df, const double* dC, int nocc, double* dJ, double* dK, int mma, int q_lo = 0,
                  int q_hi = -1);
+// Implemented in df.cu: the factor holds only a shard of the auxiliary rows.
+bool df_is_shard(const hfg_df* df);
 // Implemented in ctx.cu, used by scf.cu.
 // shard / nshards: only the shard's cost-balanced range of work-queue steps
 // of every launch (the partial J/K of all shards sum to the full build)

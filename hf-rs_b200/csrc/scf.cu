@@ -1018,6 +1018,7 @@ extern "C" int hfg_scf_df(hfg_ctx* ctx, hfg_df* df, int mma, const hfg_scf_opts*
   // CDIIS from the second iteration, convergence on |dE|, the residual and
   // max |P_next - P| of the density from the un-extrapolated Fock matrix.
   if (!ctx || !df || !o || !res) return HFG_ERR_INVALID_INPUT;
+  if (df_is_shard(df)) return set_error(ctx, HFG_ERR_INVALID_INPUT, "DF-RHF needs the whole factor, not a shard of it");
   auto t_start = std::chrono::steady_clock::now();
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);

@@ -167,6 +167,8 @@ def load_library():
     L.hfg_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, DP]
     L.hfg_scf_opts_default.argtypes = [P(SCFOptions)]
     L.hfg_df_build.argtypes = [VP, P(HfgBasis), ctypes.c_double, ctypes.c_double, ctypes.c_int, P(VP)]
+    L.hfg_df_build_shard.argtypes = [VP, P(HfgBasis), ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, P(VP)]
     L.hfg_df_destroy.argtypes = [VP]
     L.hfg_df_sizes.argtypes = [VP, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_longlong)]
     L.hfg_df_metric.argtypes = [VP, DP]
@@ -523,15 +525,18 @@ HFG_DF_FP64, HFG_DF_FP32, HFG_DF_BF16 = 0, 1, 2
 class DFTensor:
     """hfg_df: the DF factor B = X^T (P|mn) of an auxiliary basis on a context."""
 
-    def __init__(self, ctx, aux, metric_cutoff=1e-10, pair_threshold=0.0, storage=HFG_DF_FP64):
+    def __init__(self, ctx, aux, metric_cutoff=1e-10, pair_threshold=0.0, storage=HFG_DF_FP64, shard=0, nshards=1):
+        """shard/nshards: hold only that share of the whitened auxiliary
+        functions (hfg_df_build_shard), one rank's factor of a multi-GPU
+        build; its J/K are the rank's partial sums."""
         self.ctx = ctx
         self.lib = ctx.lib
         self.aux = aux
         self._b = HfgBasis(aux.n, _dp(aux.center), _ip(aux.lxyz), _ip(aux.atom), _ip(aux.prim_off), _dp(aux.exps),
                            _dp(aux.coefs))
         h = VP()
-        rc = self.lib.hfg_df_build(ctx.h, ctypes.byref(self._b), metric_cutoff, pair_threshold, storage,
-                                   ctypes.byref(h))
+        rc = self.lib.hfg_df_build_shard(ctx.h, ctypes.byref(self._b), metric_cutoff, pair_threshold, storage, shard,
+                                         nshards, ctypes.byref(h))
         ctx._check(rc)
         self.h = h
         ctx._adopt(self)

@@ -45,6 +45,19 @@ def aux_shard_range(rank, shard, nshards):
     return rank * shard // nshards, rank * (shard + 1) // nshards
 
 
+class ShardFactorDFJK(ShardedJK):
+    """DF J/K where each rank holds only its share of the factor (a DFTensor
+    built with shard=rank, nshards=world), hf-rs's map-reduce over Q
+    (src/df.rs:143-173) across GPUs: the rank's J and K over its rows, then
+    one all-reduce.  Call with (C, None, J, K) as ShardedDFJK."""
+
+    def __init__(self, rank, world, df_shard, nocc, mma=0, group=None):
+        def build(C, _unused, J, K, shard, nshards):
+            df_shard.jk_device_shard(C.data_ptr(), nocc, J.data_ptr(), K.data_ptr(), 0, 1, mma=mma)
+
+        super().__init__(rank, world, build=build, group=group)
+
+
 class ShardedDFJK(ShardedJK):
     """DF J/K of occupied coefficients on all ranks: each rank sums over its
     range of auxiliary functions (hfg_df_jk_device_shard) and one all-reduce

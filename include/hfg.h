@@ -279,6 +279,19 @@ typedef struct hfg_df hfg_df;
  */
 int hfg_df_build(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, double pair_threshold, int storage,
                  hfg_df** out);
+/*
+ * No counterpart in hf-rs (one process, Rayon over Q, src/df.rs:143-173).
+ * As hfg_df_build, but the factor holds only rows [R shard / nshards,
+ * R (shard + 1) / nshards) of the R whitened auxiliary functions: one rank's
+ * share of a multi-GPU DF build.  Every rank evaluates the three-centre
+ * integrals of all auxiliary functions; the B GEMM, the factor's memory and
+ * the J/K built from it (hfg_df_jk and its variants, which then give that
+ * rank's partial J and K, to be summed over the ranks) are divided.
+ * hfg_df_sizes reports the shard's rows.  DF-RHF and RI-MP2 need the whole
+ * factor and refuse a shard.
+ */
+int hfg_df_build_shard(hfg_ctx* ctx, const hfg_basis* aux, double metric_cutoff, double pair_threshold, int storage,
+                       int shard, int nshards, hfg_df** out);
 int hfg_df_destroy(hfg_df* df);
 int hfg_df_sizes(const hfg_df* df, int* naux, int* rank, long long* ncol);
 /* The metric (P|Q) as built (naux x naux, row-major). */

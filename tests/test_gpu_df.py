@@ -137,6 +137,40 @@ def test_df_shards_over_the_auxiliary_index_sum_to_the_full_build(mma):
     ctx.close()
 
 
+@pytest.mark.parametrize("mma", [HFG_DF_FP64, HFG_DF_BF16])
+def test_shard_factors_sum_to_the_full_build(mma):
+    # each rank of a multi-GPU DF build holds only its rows of the factor
+    # (hfg_df_build_shard); their J and K sum to the whole factor's
+    from hfgpu import HfgError
+    atoms = water_cluster(2)
+    ctx = Context(CartesianBasis.build(atoms, "cc-pvdz"))
+    aux = CartesianBasis.build(atoms, "def2-universal-jkfit")
+    storage = HFG_DF_FP64 if mma == HFG_DF_FP64 else HFG_DF_FP32
+    full = DFTensor(ctx, aux, storage=storage)
+    C = occ_coeffs(ctx.n, 10, 6)
+    J0, K0 = full.jk(C, mma=mma)
+    rank = full.sizes()[1]
+    full.close()
+    for nshards in (2, 3):
+        Js, Ks, rows = np.zeros_like(J0), np.zeros_like(K0), 0
+        for s in range(nshards):
+            d = DFTensor(ctx, aux, storage=storage, shard=s, nshards=nshards)
+            rows += d.sizes()[1]
+            J, K = d.jk(C, mma=mma)
+            Js += J
+            Ks += K
+            if s == 0:
+                with pytest.raises(HfgError, match="whole factor"):
+                    d.mp2_energy(np.eye(ctx.n), np.arange(ctx.n, dtype=float), 5)
+                with pytest.raises(HfgError, match="whole factor"):
+                    ctx.scf_df(d)
+            d.close()
+        assert rows == rank
+        tol = 1e-11 if mma == HFG_DF_FP64 else 1e-5 * np.max(np.abs(K0))
+        assert np.max(np.abs(Js - J0)) < 1e-11 and np.max(np.abs(Ks - K0)) < tol, (mma, nshards)
+    ctx.close()
+
+
 def test_df_transform_matches_the_oracle_factor_in_the_mo_basis():
     # DfTensor::transform (src/df.rs:182-210): C^T B_Q C packed over p >= q
     ctx = Context(CartesianBasis.build(ATOMS, "sto-3g"))
