@@ -605,6 +605,7 @@ void hfg_scf_opts_default(hfg_scf_opts* o) {
   o->diis_size = 8;
   o->incremental_tol = 1e-12;
   o->rebuild_every = 8;
+  o->refine_at = 10.0;
 }
 
 int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_out, double* F_out, double* C_out,
@@ -821,6 +822,7 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
     return HFG_OK;
   };
   bool refining = !mixed;
+  const double refine_at = o->refine_at > 1.0 ? o->refine_at : 1.0;
   int refine_done = 0;
   double prev_e = 0.0, e_tot = 0.0;
   bool converged = false;
@@ -867,15 +869,17 @@ int hfg_scf(hfg_ctx* ctx, const hfg_scf_opts* o, hfg_scf_result* res, double* P_
     }
     if (o->verbose) fprintf(stderr, "hfg scf %3d  E = %.12f  dE = %.3e  |e| = %.3e  dP = %.3e  %s\n", it, e_tot, de, en, dr,
                            refining ? "fp64" : "mixed");
-    if (it > 1 && de < o->energy_tol && en < o->residual_tol && dr < o->density_tol) {
-      if (refining && refine_done >= (mixed ? std::max(1, o->refine_iters) : 0)) {
-        converged = true;
-        break;
-      }
-      if (!refining) {
-        res->energy_before_refinement = e_tot;
-        refining = true;
-      }
+    if (it > 1 && de < o->energy_tol && en < o->residual_tol && dr < o->density_tol &&
+        refining && refine_done >= (mixed ? std::max(1, o->refine_iters) : 0)) {
+      converged = true;
+      break;
+    }
+    // the mixed phase ends once the measures are below refine_at x the
+    // tolerances (refine_at = 1: fully converged in mixed precision)
+    if (!refining && it > 1 && de < refine_at * o->energy_tol && en < refine_at * o->residual_tol &&
+        dr < refine_at * o->density_tol) {
+      res->energy_before_refinement = e_tot;
+      refining = true;
     }
     if (mixed && !refining && it >= o->max_iter - std::max(1, o->refine_iters)) {
       res->energy_before_refinement = e_tot;

@@ -57,7 +57,8 @@ class SCFOptions(ctypes.Structure):
                 ("max_iter", ctypes.c_int), ("energy_tol", ctypes.c_double), ("residual_tol", ctypes.c_double),
                 ("density_tol", ctypes.c_double), ("jk", JKOptions), ("refine_iters", ctypes.c_int),
                 ("diis_size", ctypes.c_int), ("verbose", ctypes.c_int), ("guess", ctypes.c_int),
-                ("incremental_tol", ctypes.c_double), ("rebuild_every", ctypes.c_int)]
+                ("incremental_tol", ctypes.c_double), ("rebuild_every", ctypes.c_int),
+                ("refine_at", ctypes.c_double)]
 
 
 class SCFResult(ctypes.Structure):
@@ -386,7 +387,8 @@ class Context:
         return Fa, Fb
 
     def scf(self, charge=0, multiplicity=1, uhf=False, spherical=False, tol=1e-10, max_iter=100, jk=None,
-            refine_iters=2, verbose=False, want=("P", "F"), guess="sad", incremental=1e-12, rebuild_every=8):
+            refine_iters=2, verbose=False, want=("P", "F"), guess="sad", incremental=1e-12, rebuild_every=8,
+            refine_at=10.0):
         """Device SCF (hfg_scf) for the context's molecule; returns a dict.
         `incremental` (mixed J/K only): screening tolerance of the builds from
         density changes, 0 for a full build every iteration."""
@@ -407,6 +409,7 @@ class Context:
         o.guess = 0 if guess == "sad" else 1
         o.incremental_tol = incremental
         o.rebuild_every = rebuild_every
+        o.refine_at = refine_at
         n = self.n
         ns = 2 if uhf else 1
         P = np.zeros((ns, n, n)) if "P" in want else None

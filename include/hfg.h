@@ -389,6 +389,9 @@ typedef struct {
                               last full build, skipping shell quartets with Q_ab Q_cd max|dP| below
                               this (1e-12 by default; 0: a full build every iteration) */
   int rebuild_every;       /* full build after this many incremental ones (default 8) */
+  double refine_at;        /* HFG_MIXED: the FP64 refinement starts once the three convergence
+                              measures are below refine_at times their tolerances (default 10;
+                              1: the mixed phase converges fully first) */
 } hfg_scf_opts;
 
 typedef struct {
