@@ -313,7 +313,7 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"jk_only": True, "waters": args.waters, "builds": args.warmup + args.steps}))
         return
-    # mixed form chosen by the autotuner (FP32 threshold 1e-9..1e-6, primitive
+    # mixed form chosen by the autotuner (FP32 threshold 1e-7..1e-4, primitive
     # threshold 1e-15..1e-13, build energy error within 5e-9 Eh of the plain
     # FP64 build); untimed
     opt_mixed, tune = ctx.autotune(P.data_ptr(), P.data_ptr(), base=JKOptions.make(schwarz=SCHWARZ),
@@ -458,7 +458,8 @@ def run_ours(args):
     scfres = None
     scf_waters = args.waters if args.scf_waters < 0 else args.scf_waters
     if world == 1 and scf_waters > 0:
-        scfres = measure_scf(scf_waters, ctx if scf_waters == args.waters else None, opt_mixed)
+        from hfgpu.serve import MIXED
+        scfres = measure_scf(scf_waters, ctx if scf_waters == args.waters else None, MIXED)
     mt, pt, tl = opt_mixed.mixed_threshold, opt_mixed.prim_threshold, opt_mixed.tile or 64
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_mixed / args.steps, "higher_is_better": True,
@@ -528,9 +529,10 @@ def measure_serving(args):
 def measure_scf(waters, ctx, opt_mixed):
     """Full SCF of (H2O)_n cc-pVDZ (spherical AO space, tol 1e-10, SAD start,
     CDIIS): FP64 builds with primitive screening 1e-15, and the mixed form
-    (incremental builds, FP64 refinement of at least two builds).  Reports
-    both energies, the mixed energy's error and the error before refinement,
-    iterations and wall times (basis to converged energy)."""
+    tuned for whole SCFs (hfgpu.serve.MIXED; incremental builds, FP64
+    refinement of at least two builds).  Reports both energies, the mixed
+    energy's error and the error before refinement, iterations and wall
+    times (basis to converged energy)."""
     from hfgpu import CartesianBasis, Context, JKOptions
     from hfgpu.clusters import water_cluster
     own = ctx is None

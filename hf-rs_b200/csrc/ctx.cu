@@ -1507,7 +1507,7 @@ int hfg_fock_uhf(hfg_ctx* ctx, const hfg_jk_opts* opts, const double* H, const d
 
 void hfg_autotune_opts_default(hfg_autotune_opts* o) {
   *o = hfg_autotune_opts{};
-  const double f[4] = {1e-9, 1e-8, 1e-7, 1e-6}, p[3] = {1e-15, 1e-14, 1e-13};
+  const double f[4] = {1e-7, 1e-6, 1e-5, 1e-4}, p[3] = {1e-15, 1e-14, 1e-13};
   for (int i = 0; i < 4; ++i) o->fp32_thresholds[i] = f[i];
   o->n_fp32 = 4;
   for (int i = 0; i < 3; ++i) o->prim_thresholds[i] = p[i];

@@ -86,6 +86,10 @@ def summarize(results, makespan):
             "failed": int(sum(r["status"] not in (0,) for r in results))}
 
 
-# the served mixed form: the thresholds the autotuner picks on (H2O)64
-# cc-pVDZ (build energy error ~1e-9 Eh there; the FP64 refinement removes it)
-MIXED = JKOptions.make(prim=1e-13, mixed=1e-6)
+# the mixed form for whole SCFs (served jobs, the SCF bench leg): FP32
+# below Q_ab Q_cd < 3e-5, primitive screening 1e-13.  Swept on (H2O)32 and
+# (H2O)48 cc-pVDZ SCFs it keeps the FP64 iteration count and is fastest;
+# larger FP32 thresholds win single builds but cost SCF iterations (1e-4:
+# 21-33 iterations instead of 18).  Build energy error ~2e-9 Eh at (H2O)64;
+# the FP64 refinement removes it.
+MIXED = JKOptions.make(prim=1e-13, mixed=3e-5)
