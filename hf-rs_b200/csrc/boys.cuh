@@ -20,9 +20,9 @@
 //    changes F_m by less than 1e-13 relative and is dropped.
 //
 // The FP32 flavour (only for quartets with small Schwarz bounds) uses an
-// order-4 Taylor row F_L/k!, k = 0..4 plus e^{-T0} and __expf for T <= 36
-// (truncation below 1e-9 relative); for T > 36 it evaluates the FP64 branch
-// above and rounds each F_m to FP32.
+// order-4 Taylor row F_L/k!, k = 0..4 plus e^{-T0}, and an order-4 Taylor of
+// e^{-dT}, for T <= 36 (truncation below 1e-9 relative); for T > 36 it
+// evaluates the FP64 branch above and rounds each F_m to FP32.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -128,15 +128,25 @@ __device__ __forceinline__ void boys_eval(float t, const float* __restrict__ sm,
     }
     return;
   }
-  const int idx = min(max(__float2int_rn(t * 20.0f), 0), kBoysSmemRows - 1);
-  const float x = idx * 0.05f - t;
+  // nearest grid point by adding and subtracting 1.5 * 2^23, which rounds
+  // 20 t (0 <= 20 t <= 720 here) to an integer in the FP32 adder and leaves
+  // it in the low mantissa bits; no float<->int conversions (the clamp also
+  // catches a NaN t)
+  const float y = t * 20.0f + 12582912.0f;
+  const int idx = min(max(__float_as_int(y) - 0x4B400000, 0), kBoysSmemRows - 1);
+  const float x = (y - 12582912.0f) * 0.05f - t;
   const float* row = sm + idx * 7;
   float acc = fmaf(row[4], x, row[3]);
   acc = fmaf(acc, x, row[2]);
   acc = fmaf(acc, x, row[1]);
   F[L] = fmaf(acc, x, row[0]);
   if (L > 0) {
-    const float e = row[5] * __expf(x);
+    // e^{x}, |x| <= 0.025: order-4 Taylor (truncation below 1e-10 relative)
+    float ex = fmaf(x, 1.0f / 24.0f, 1.0f / 6.0f);
+    ex = fmaf(ex, x, 0.5f);
+    ex = fmaf(ex, x, 1.0f);
+    ex = fmaf(ex, x, 1.0f);
+    const float e = row[5] * ex;
     const float t2 = 2.0f * t;
 #pragma unroll
     for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0f / (2 * m + 1));

@@ -616,6 +616,16 @@ __global__ void symmetrize_kernel(const double* __restrict__ acc, double* __rest
   out[t] = 0.5 * (acc[m * nn + (long long)i * n + j] + acc[m * nn + (long long)j * n + i]);
 }
 
+// FP32 copies of the densities for the FP32 launches: out[0, nn) = Pt,
+// out[nn, nn + nspin nn) = Ps.
+__global__ void densities_to_f32_kernel(const double* __restrict__ Pt, const double* __restrict__ Ps,
+                                        float* __restrict__ out, long long nn, int nspin) {
+  const long long total = nn * (1 + nspin);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    out[t] = (float)(t < nn ? Pt[t] : Ps[t - nn]);
+}
+
 // One matrix of a batched build: its accumulator and (symmetrised) output.
 struct BatchMat {
   double* acc;
@@ -690,6 +700,12 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   HFG_CUDA(ctx, ctx->d_Jacc.alloc(nn));
   HFG_CUDA(ctx, ctx->d_Kacc.alloc(2 * nn));
   HFG_CUDA(ctx, ctx->d_counters.alloc(plan->launches.size() + 1));
+  // FP32 launches read FP32 copies of the densities, made at the start of
+  // the build; the buffer is sized for UHF from the first use on, so it never
+  // moves under a captured graph
+  bool any32 = false;
+  for (const Launch& L : plan->launches) any32 = any32 || L.fp32;
+  if (any32) HFG_CUDA(ctx, ctx->d_D32.alloc(3 * nn));
   // HFG_PROFILE=1: per-launch device time (CUDA events) on stderr
   static const bool profile = getenv("HFG_PROFILE") && getenv("HFG_PROFILE")[0] == '1';
   // The build is a fixed sequence (clears, one launch per class, two
@@ -724,6 +740,8 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   a.expt32 = ctx->d_expt32.p;
   a.Dtot = dPt;
   a.Dspin = dPs;
+  a.Dtot32 = any32 ? ctx->d_D32.p : nullptr;
+  a.Dspin32 = any32 ? ctx->d_D32.p + nn : nullptr;
   a.Jacc = ctx->d_Jacc.p;
   a.Kacc = ctx->d_Kacc.p;
   a.n = ctx->n;
@@ -731,6 +749,12 @@ int jk_device_locked(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const dou
   a.prim_eps = o.prim_threshold;
   a.serial = o.deterministic != 0;
   auto enqueue = [&]() -> int {
+  if (any32) {
+    const long long tot = (long long)nn * (1 + nspin);
+    densities_to_f32_kernel<<<(unsigned)std::min<long long>((tot + 255) / 256, 148 * 8), 256, 0, ctx->stream>>>(
+        dPt, dPs, ctx->d_D32.p, (long long)nn, nspin);
+    HFG_CUDA(ctx, cudaGetLastError());
+  }
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Jacc.p, 0, nn * sizeof(double), ctx->stream));
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_Kacc.p, 0, nspin * nn * sizeof(double), ctx->stream));
   HFG_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.p, 0, (plan->launches.size() + 1) * 8, ctx->stream));
@@ -876,6 +900,7 @@ hfg_ctx::~hfg_ctx() {
   d_counters.release();
   d_D.release();
   d_Ds.release();
+  d_D32.release();
   d_Jacc.release();
   d_Kacc.release();
   d_J.release();

@@ -166,6 +166,7 @@ struct hfg_ctx {
   hfg::DevBuf<float> d_boys32, d_expt32;
   hfg::DevBuf<unsigned long long> d_counters;  // one work-queue counter per J/K launch
   hfg::DevBuf<double> d_D, d_Ds, d_Jacc, d_Kacc, d_J, d_K, d_tmp;
+  hfg::DevBuf<float> d_D32;  // FP32 copies of a build's densities (3 n^2)
 
   // launch plans by (Schwarz, FP32 and primitive thresholds, precision, tile)
   std::map<std::tuple<double, double, double, int, int>, std::unique_ptr<hfg::Plan>> plans;

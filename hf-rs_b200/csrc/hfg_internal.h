@@ -104,6 +104,10 @@ struct JKLaunchArgs {
   unsigned long long* counter;  // work-queue counter of this launch (zeroed before it)
   const double* Dtot;  // n x n
   const double* Dspin; // nspin n x n
+  // FP32 copies of Dtot / Dspin for the FP32 launches (null: they round the
+  // FP64 densities as they load them)
+  const float* Dtot32;
+  const float* Dspin32;
   double* Jacc;        // n x n
   double* Kacc;        // nspin n x n
   int n, nspin;

@@ -45,19 +45,31 @@ struct DBlocks {
   DT cd[NC * ND], ab[NA * NB];
   DT bd[NS][NB * ND], ad[NS][NA * ND], bc[NS][NB * NC], ac[NS][NA * NC];
   __device__ __forceinline__ void load(const PairInfo& bra, const PairInfo& ket, const JKLaunchArgs& a) {
-    const int n = a.n;
+    // FP32 launches read the build's FP32 copies when it made them (half the
+    // bytes, no conversions)
+    if constexpr (sizeof(DT) == 4) {
+      if (a.Dtot32) {
+        fill(bra, ket, a.n, a.Dtot32, a.Dspin32);
+        return;
+      }
+    }
+    fill(bra, ket, a.n, a.Dtot, a.Dspin);
+  }
+  template <typename ST>
+  __device__ __forceinline__ void fill(const PairInfo& bra, const PairInfo& ket, int n, const ST* __restrict__ Dt,
+                                       const ST* __restrict__ Ds) {
     const int i0 = bra.ao_a, j0 = bra.ao_b, k0 = ket.ao_a, l0 = ket.ao_b;
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
-      for (int l = 0; l < ND; ++l) cd[k * ND + l] = (DT)__ldg(a.Dtot + (size_t)(k0 + k) * n + l0 + l);
+      for (int l = 0; l < ND; ++l) cd[k * ND + l] = (DT)__ldg(Dt + (size_t)(k0 + k) * n + l0 + l);
 #pragma unroll
     for (int i = 0; i < NA; ++i)
 #pragma unroll
-      for (int j = 0; j < NB; ++j) ab[i * NB + j] = (DT)__ldg(a.Dtot + (size_t)(i0 + i) * n + j0 + j);
+      for (int j = 0; j < NB; ++j) ab[i * NB + j] = (DT)__ldg(Dt + (size_t)(i0 + i) * n + j0 + j);
 #pragma unroll
     for (int sp = 0; sp < NS; ++sp) {
-      const double* D = a.Dspin + (size_t)sp * n * n;
+      const ST* D = Ds + (size_t)sp * n * n;
 #pragma unroll
       for (int j = 0; j < NB; ++j)
 #pragma unroll
@@ -466,6 +478,8 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
     la.pbound = jb.pbound;
     la.Dtot = jb.Dtot;
     la.Dspin = jb.Dtot;
+    la.Dtot32 = nullptr;
+    la.Dspin32 = nullptr;
     la.Jacc = jb.Jacc;
     la.Kacc = jb.Kacc;
     la.n = jb.n;
