@@ -1174,6 +1174,11 @@ int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, c
     const size_t nn = (size_t)c->n * c->n;
     BK(c->d_Jacc.alloc(nn));
     BK(c->d_Kacc.alloc(2 * nn));
+    for (const Launch& L : plans[j]->launches)
+      if (L.fp32) {
+        BK(c->d_D32.alloc(3 * nn));
+        break;
+      }
     BK(c->ensure_side_streams());
     if (c->stream != st) {
       BK(cudaEventRecord(c->ev_fork, c->stream));
@@ -1255,6 +1260,7 @@ int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, c
       x.rec32 = c->d_rec32.p;
       x.pbound = c->d_pbound.p;
       x.Dtot = d_P[j];
+      x.Dtot32 = c->d_D32.p;
       x.Jacc = c->d_Jacc.p;
       x.Kacc = c->d_Kacc.p;
       x.thr = opts[j].schwarz_threshold;
@@ -1279,6 +1285,16 @@ int jk_batch_locked(hfg_ctx* const* ctxs, int n_jobs, const hfg_jk_opts* opts, c
   const dim3 mgrid((unsigned)std::min<long long>((nnmax + 255) / 256, 64), (unsigned)(2 * n_jobs));
   batch_mats_kernel<<<mgrid, 256, 0, st>>>(d_mats, 0);
   BK(cudaGetLastError());
+  // FP32 copies of the densities of the molecules with FP32 launches
+  for (int j = 0; j < n_jobs; ++j) {
+    bool any32 = false;
+    for (const Launch& L : plans[j]->launches) any32 = any32 || (L.fp32 && L.nchunks > 0);
+    if (!any32) continue;
+    const long long nn = (long long)ctxs[j]->n * ctxs[j]->n;
+    densities_to_f32_kernel<<<(unsigned)std::min<long long>((nn + 255) / 256, 148 * 8), 256, 0, st>>>(
+        d_P[j], d_P[j], ctxs[j]->d_D32.p, nn, 0);
+    BK(cudaGetLastError());
+  }
   // the groups run concurrently over the first context's side streams
   BK(cudaEventRecord(c0->ev_fork, st));
   for (int k = 0; k < kJKSideStreams; ++k) BK(cudaStreamWaitEvent(c0->side[k], c0->ev_fork, 0));

@@ -76,6 +76,7 @@ struct JKJob {
   const float* pbound;
   KetSoA kets;
   const double* Dtot;
+  const float* Dtot32;  // its FP32 copy (FP32 launches)
   double* Jacc;
   double* Kacc;
   double thr, prim_eps;  // the molecule's Schwarz and primitive thresholds
@@ -104,8 +105,8 @@ struct JKLaunchArgs {
   unsigned long long* counter;  // work-queue counter of this launch (zeroed before it)
   const double* Dtot;  // n x n
   const double* Dspin; // nspin n x n
-  // FP32 copies of Dtot / Dspin for the FP32 launches (null: they round the
-  // FP64 densities as they load them)
+  // FP32 copies of Dtot / Dspin, read by the FP32 launches (required for
+  // them)
   const float* Dtot32;
   const float* Dspin32;
   double* Jacc;        // n x n

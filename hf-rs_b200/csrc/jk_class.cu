@@ -37,6 +37,9 @@ static cudaError_t launch_t(const JKLaunchArgs& a, cudaStream_t st) {
     resident = sms * (per_sm > 0 ? per_sm : 1);
     if (dev >= 0 && dev < kMaxDev) resident_by_dev[dev].store(resident, std::memory_order_relaxed);
   }
+  // FP32 launches read the FP32 density copies (a batched launch carries
+  // them in its molecule table)
+  if (sizeof(T) == 4 && !BATCH && (!a.Dtot32 || (NS == 2 && !a.Dspin32))) return cudaErrorInvalidValue;
   if (a.serial) {
     if (a.nchunks > 0) kern<<<1, 32, smem, st>>>(a);
     return cudaGetLastError();

@@ -45,15 +45,10 @@ struct DBlocks {
   DT cd[NC * ND], ab[NA * NB];
   DT bd[NS][NB * ND], ad[NS][NA * ND], bc[NS][NB * NC], ac[NS][NA * NC];
   __device__ __forceinline__ void load(const PairInfo& bra, const PairInfo& ket, const JKLaunchArgs& a) {
-    // FP32 launches read the build's FP32 copies when it made them (half the
-    // bytes, no conversions)
-    if constexpr (sizeof(DT) == 4) {
-      if (a.Dtot32) {
-        fill(bra, ket, a.n, a.Dtot32, a.Dspin32);
-        return;
-      }
-    }
-    fill(bra, ket, a.n, a.Dtot, a.Dspin);
+    // FP32 launches read the build's FP32 copies (half the bytes, no
+    // conversions); their launcher refuses to start without them
+    if constexpr (sizeof(DT) == 4) fill(bra, ket, a.n, a.Dtot32, a.Dspin32);
+    else fill(bra, ket, a.n, a.Dtot, a.Dspin);
   }
   template <typename ST>
   __device__ __forceinline__ void fill(const PairInfo& bra, const PairInfo& ket, int n, const ST* __restrict__ Dt,
@@ -478,8 +473,8 @@ __global__ void __launch_bounds__(256, (MinBlocks<LA, LB, LC, LD, T>::value)) jk
     la.pbound = jb.pbound;
     la.Dtot = jb.Dtot;
     la.Dspin = jb.Dtot;
-    la.Dtot32 = nullptr;
-    la.Dspin32 = nullptr;
+    la.Dtot32 = jb.Dtot32;
+    la.Dspin32 = jb.Dtot32;
     la.Jacc = jb.Jacc;
     la.Kacc = jb.Kacc;
     la.n = jb.n;

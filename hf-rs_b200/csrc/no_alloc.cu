@@ -13,9 +13,11 @@
 //
 // Limit: the array holds 8 MiB: the plan's work-queue counters (8 bytes per
 // launch, rounded up to 256 bytes) plus (1 + nspin) * n^2 doubles of
-// accumulators, so n <= 724 for RHF and n <= 591 for UHF (for plans of up to
-// 224 launches; an s/p/d basis needs at most 42).  Larger systems are
-// rejected with HFG_ERR_INVALID_INPUT.
+// accumulators, and for plans with FP32 launches (mixed precision)
+// (1 + nspin) * n^2 floats of FP32 density copies.  So n <= 724 for RHF and
+// n <= 591 for UHF in FP64, n <= 591 and n <= 482 in mixed precision (for
+// plans of up to 224 launches; an s/p/d basis needs at most 42).  Larger
+// systems are rejected with HFG_ERR_INVALID_INPUT.
 //
 // The first call on a device looks up the array's device address (once per
 // device, with that device current); make that first call before any stream
@@ -65,6 +67,14 @@ __global__ void symmetrize_noalloc(const double* __restrict__ acc, double* __res
   out[t] = 0.5 * (acc[m * nn + (long long)i * n + j] + acc[m * nn + (long long)j * n + i]);
 }
 
+// FP32 copies of the densities for the FP32 launches of a mixed plan.
+__global__ void densities_f32_noalloc(const double* __restrict__ Pt, const double* __restrict__ Ps,
+                                      float* __restrict__ out, long long nn, int nspin) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nn * (1 + nspin)) return;
+  out[t] = (float)(t < nn ? Pt[t] : Ps[t - nn]);
+}
+
 }  // namespace
 
 extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double* dPt,
@@ -82,8 +92,9 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
     return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, "invalid J/K options");
   const size_t nn = (size_t)ctx->n * ctx->n;
   const char* too_big =
-      "hfg_jk_device_noalloc: (1 + nspin) * n^2 doubles and the work-queue counters exceed its 8 MiB scratch "
-      "(n <= 724 for RHF, n <= 591 for UHF); use hfg_jk_device";
+      "hfg_jk_device_noalloc: (1 + nspin) * n^2 doubles (and in mixed precision (1 + nspin) * n^2 floats) and the "
+      "work-queue counters exceed its 8 MiB scratch (n <= 724 for RHF, n <= 591 for UHF; mixed precision n <= 591 "
+      "and n <= 482); use hfg_jk_device";
   if (256 + (size_t)(1 + nspin) * nn * sizeof(double) > kScratchBytes)
     return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, too_big);
   std::lock_guard<std::mutex> lk(ctx->mu);
@@ -97,7 +108,11 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
   // counters first (one per launch, rounded up to keep the accumulators
   // 256-byte aligned), then J' and K'
   const size_t counter_bytes = (plan.launches.size() * sizeof(unsigned long long) + 255) / 256 * 256;
-  const size_t need = counter_bytes + (size_t)(1 + nspin) * nn * sizeof(double);
+  const size_t acc_bytes = (size_t)(1 + nspin) * nn * sizeof(double);
+  bool any32 = false;
+  for (const hfg::Launch& L : plan.launches) any32 = any32 || L.fp32;
+  const size_t f32_bytes = any32 ? (size_t)(1 + nspin) * nn * sizeof(float) : 0;
+  const size_t need = counter_bytes + acc_bytes + f32_bytes;
   if (need > kScratchBytes) return hfg::set_error(ctx, HFG_ERR_INVALID_INPUT, too_big);
   if (cudaSetDevice(ctx->device) != cudaSuccess) return hfg::set_error(ctx, HFG_ERR_CUDA, "cudaSetDevice");
   void* base = nullptr;
@@ -107,9 +122,17 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
   unsigned long long* counters = reinterpret_cast<unsigned long long*>(b);
   double* Jacc = reinterpret_cast<double*>(b + counter_bytes);
   double* Kacc = Jacc + nn;
+  float* D32 = reinterpret_cast<float*>(b + counter_bytes + acc_bytes);
   // the array keeps the last call's contents: clear counters and accumulators
-  rc = hfg::cuda_check(ctx, cudaMemsetAsync(b, 0, need, ctx->stream), "scratch clear");
+  rc = hfg::cuda_check(ctx, cudaMemsetAsync(b, 0, counter_bytes + acc_bytes, ctx->stream), "scratch clear");
   if (rc != HFG_OK) return rc;
+  if (any32) {
+    const long long tot = (long long)nn * (1 + nspin);
+    densities_f32_noalloc<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(dPt, dPs, D32, (long long)nn,
+                                                                                  nspin);
+    rc = hfg::cuda_check(ctx, cudaGetLastError(), "FP32 densities");
+    if (rc != HFG_OK) return rc;
+  }
   hfg::JKLaunchArgs a{};
   a.pairs = ctx->d_pairs.p;
   a.kets = ctx->kets();
@@ -124,6 +147,8 @@ extern "C" int hfg_jk_device_noalloc(hfg_ctx* ctx, const hfg_jk_opts* opts, int 
   a.expt32 = ctx->d_expt32.p;
   a.Dtot = dPt;
   a.Dspin = dPs;
+  a.Dtot32 = any32 ? D32 : nullptr;
+  a.Dspin32 = any32 ? D32 + nn : nullptr;
   a.Jacc = Jacc;
   a.Kacc = Kacc;
   a.n = ctx->n;

@@ -147,9 +147,10 @@ int hfg_jk_device(hfg_ctx* ctx, const hfg_jk_opts* opts, int nspin, const double
  * and host programs whose own allocator has reserved all device memory.
  * The J'/K' accumulators and work-queue counters live in one 8 MiB device
  * array that the library reserves when it is loaded, so (1 + nspin) * n^2
- * doubles plus 8 bytes per launch of the plan (rounded up to 256) must fit:
- * n <= 724 (RHF), n <= 591 (UHF); larger systems return
- * HFG_ERR_INVALID_INPUT.  The launch plan for `opts` must already exist on
+ * doubles plus 8 bytes per launch of the plan (rounded up to 256), and in
+ * mixed precision (1 + nspin) * n^2 floats of FP32 density copies, must fit:
+ * n <= 724 (RHF), n <= 591 (UHF) in FP64, n <= 591 (RHF), n <= 482 (UHF) in
+ * mixed precision; larger systems return HFG_ERR_INVALID_INPUT.  The launch plan for `opts` must already exist on
  * the context (one earlier hfg_jk or hfg_jk_device call with the same
  * options builds it).  The first call on a device looks up the array's
  * device address; make that first call before any stream capture.  All calls
