@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-jobs", type=int, default=16)
     ap.add_argument("--serve-max-waters", type=int, default=48)
-    ap.add_argument("--df-waters", type=int, default=48, help="also time DF J/K on (H2O)_n (0: skip)")
+    ap.add_argument("--df-waters", type=int, default=128,
+                    help="also time DF J/K on (H2O)_n (0: skip; default the DF-RHF workload, (H2O)128)")
     ap.add_argument("--scf-waters", type=int, default=-1,
                     help="full SCF in FP64 and in the mixed form on (H2O)_n (-1: --waters, 0: skip)")
     ap.add_argument("--jk-only", action="store_true",
@@ -496,7 +497,9 @@ def run_ours(args):
                                                            round(serving["served_mixed_8_slots"]["p99_s"], 3)],
         "scf_mixed_minus_fp64_eh": None if scfres is None else scfres["mixed_minus_fp64_eh"],
         "scf_before_refinement_minus_fp64_eh": None if scfres is None else scfres["before_refinement_minus_fp64_eh"],
-        "df_k_tflops": None if dfres is None else dfres.get("k_tflops_best")}
+        "df_k_tflops": None if dfres is None else dfres.get("k_tflops_best"),
+        "df_waters": None if dfres is None else dfres.get("waters"),
+        "df_bf16_tensor_frac": None if dfres is None else dfres.get("bf16", {}).get("tensor_peak_frac")}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
