@@ -40,14 +40,16 @@ template <> __device__ __forceinline__ double rsqrt_t<double>(double x) { return
 template <> __device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
 
 // One primitive quartet added into acc: bra primitive pair (p, 1/p, kp,
-// P - A) and ket primitive pair (q, 1/q, kq, Q - C); AC = A - C.
+// P - A) and ket primitive pair (q, 1/q, ckq = 2 pi^{5/2} kq, Q - C), with
+// ACQ = (A - C) - (Q - C), so that P - Q = (P - A) + ACQ.  The ket-side
+// terms are formed once per ket primitive pair by the callers' outer loops.
 template <int LA, int LB, int LC, int LD, typename T>
-__device__ __forceinline__ void prim_quartet(T* __restrict__ acc, T p, T inv_p, T kpp, T PAx, T PAy, T PAz, T q,
-                                             T inv_q, T kpq, T QCx, T QCy, T QCz, T ACx, T ACy, T ACz,
-                                             const T* __restrict__ sm) {
+__device__ __forceinline__ void prim_quartet_k(T* __restrict__ acc, T p, T inv_p, T kpp, T PAx, T PAy, T PAz, T q,
+                                               T inv_q, T ckq, T QCx, T QCy, T QCz, T ACQx, T ACQy, T ACQz,
+                                               const T* __restrict__ sm) {
   using C = EriClass<LA, LB, LC, LD>;
   constexpr int L = C::L;
-  const T PQx = ACx + PAx - QCx, PQy = ACy + PAy - QCy, PQz = ACz + PAz - QCz;
+  const T PQx = PAx + ACQx, PQy = PAy + ACQy, PQz = PAz + ACQz;
   const T s = p + q;
   const T r = rsqrt_t<T>(s);
   const T inv_s = r * r;
@@ -55,12 +57,21 @@ __device__ __forceinline__ void prim_quartet(T* __restrict__ acc, T p, T inv_p, 
   const T tt = pq_s * (PQx * PQx + PQy * PQy + PQz * PQz);
   T F[L + 1];
   boys_eval<L>(tt, sm, F);
-  const T pref = (T)kTwoPiPow25 * kpp * kpq * r;
+  const T pref = kpp * ckq * r;
 #pragma unroll
   for (int m = 0; m <= L; ++m) F[m] *= pref;
   const T qs = q * inv_s, ps = p * inv_s;
   C::prim(acc, F, PAx, PAy, PAz, -qs * PQx, -qs * PQy, -qs * PQz, QCx, QCy, QCz, ps * PQx, ps * PQy, ps * PQz,
           (T)0.5 * inv_p, (T)0.5 * inv_q, (T)0.5 * inv_s, qs, ps);
+}
+
+// The same from A - C and the ket's kq, for callers without an outer ket loop.
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void prim_quartet(T* __restrict__ acc, T p, T inv_p, T kpp, T PAx, T PAy, T PAz, T q,
+                                             T inv_q, T kpq, T QCx, T QCy, T QCz, T ACx, T ACy, T ACz,
+                                             const T* __restrict__ sm) {
+  prim_quartet_k<LA, LB, LC, LD, T>(acc, p, inv_p, kpp, PAx, PAy, PAz, q, inv_q, (T)kTwoPiPow25 * kpq, QCx, QCy, QCz,
+                                    ACx - QCx, ACy - QCy, ACz - QCz, sm);
 }
 
 template <int LA, int LB, int LC, int LD>

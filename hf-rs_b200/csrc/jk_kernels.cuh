@@ -206,15 +206,23 @@ __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefe
 
 // K'[a,c], K'[b,c] of FP32 launches are summed over the lanes that share the
 // ket's first shell c before their atomics (kets are ordered by AO index
-// within each Schwarz bucket, so such lanes are neighbours); FP64 launches
-// add them per lane.  HFG_JK_SEG_F64=1 / HFG_JK_SEG_F32=0 override this in
+// within each Schwarz bucket, so such lanes are neighbours).  FP64 launches
+// do the same for the classes where it measured faster ((10|10), (11|10),
+// (20|10): 4-12% each in an FP64 build of (H2O)64 cc-pVDZ) and add per lane
+// otherwise.  HFG_JK_SEG_F64=0/1 and HFG_JK_SEG_F32=0 override this in
 // tuning builds.
 #ifndef HFG_JK_SEG_F64
-#define HFG_JK_SEG_F64 0
+#define HFG_JK_SEG_F64 -1
 #endif
 #ifndef HFG_JK_SEG_F32
 #define HFG_JK_SEG_F32 1
 #endif
+template <int LA, int LB, int LC, int LD, typename T> struct SegReduce {
+  static constexpr int code = LA * 1000 + LB * 100 + LC * 10 + LD;
+  static constexpr bool f64_table = code == 1010 || code == 1110 || code == 2010;
+  static constexpr bool value =
+      sizeof(T) == 4 ? HFG_JK_SEG_F32 != 0 : (HFG_JK_SEG_F64 < 0 ? f64_table : HFG_JK_SEG_F64 != 0);
+};
 
 // Sum of v over this lane's run of lanes [lane, end), left in the run's
 // first lane (segmented tree over contiguous runs of at most 32 lanes).
@@ -236,7 +244,7 @@ __device__ __forceinline__ T run_sum(T v, int lane, int end) {
 template <int LA, int LB, int LC, int LD, typename T, int NS>
 __device__ __forceinline__ void jk_step(const JKLaunchArgs& a, long long c, int lane, const T* __restrict__ sm) {
   using C = EriClass<LA, LB, LC, LD>;
-  constexpr bool SEG = sizeof(T) == 4 ? HFG_JK_SEG_F32 : HFG_JK_SEG_F64;
+  constexpr bool SEG = SegReduce<LA, LB, LC, LD, T>::value;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
   {
     const long long t0 = __ldg(a.chunk_start + c), t1 = __ldg(a.chunk_start + c + 1);
@@ -313,6 +321,8 @@ __device__ __forceinline__ void jk_step(const JKLaunchArgs& a, long long c, int 
               qbn = kb[(ik + 1) * ks];
             }
             const T QCx = -Q.bp * kABx, QCy = -Q.bp * kABy, QCz = -Q.bp * kABz;
+            const T ACQx = ACx - QCx, ACQy = ACy - QCy, ACQz = ACz - QCz;
+            const T ckq = (T)kTwoPiPow25 * Q.kp;
             int ib = 0;
             if constexpr (C::NACC <= 9) {
               // two independent primitive quartets per step (bra primitive pairs
@@ -320,18 +330,20 @@ __device__ __forceinline__ void jk_step(const JKLaunchArgs& a, long long c, int 
               for (; ib + 1 < nb; ib += 2) {
                 if (bb[(ib + 1) * bs] * qb < eps) break;
                 const Rec P0 = br[ib * bs], P1 = br[(ib + 1) * bs];
-                prim_quartet<LA, LB, LC, LD, T>(acc, P0.p, P0.inv_p, P0.kp, -P0.bp * bABx, -P0.bp * bABy,
-                                                -P0.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
-                prim_quartet<LA, LB, LC, LD, T>(acc, P1.p, P1.inv_p, P1.kp, -P1.bp * bABx, -P1.bp * bABy,
-                                                -P1.bp * bABz, Q.p, Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
+                prim_quartet_k<LA, LB, LC, LD, T>(acc, P0.p, P0.inv_p, P0.kp, -P0.bp * bABx, -P0.bp * bABy,
+                                                  -P0.bp * bABz, Q.p, Q.inv_p, ckq, QCx, QCy, QCz, ACQx, ACQy, ACQz,
+                                                  sm);
+                prim_quartet_k<LA, LB, LC, LD, T>(acc, P1.p, P1.inv_p, P1.kp, -P1.bp * bABx, -P1.bp * bABy,
+                                                  -P1.bp * bABz, Q.p, Q.inv_p, ckq, QCx, QCy, QCz, ACQx, ACQy, ACQz,
+                                                  sm);
               }
             }
             Rec P = br[(ib < nb ? ib : 0) * bs];
             for (; ib < nb; ++ib) {
               const Rec Pn = br[(ib + 1 < nb ? ib + 1 : ib) * bs];
               if (bb[ib * bs] * qb < eps) break;
-              prim_quartet<LA, LB, LC, LD, T>(acc, P.p, P.inv_p, P.kp, -P.bp * bABx, -P.bp * bABy, -P.bp * bABz, Q.p,
-                                              Q.inv_p, Q.kp, QCx, QCy, QCz, ACx, ACy, ACz, sm);
+              prim_quartet_k<LA, LB, LC, LD, T>(acc, P.p, P.inv_p, P.kp, -P.bp * bABx, -P.bp * bABy, -P.bp * bABz,
+                                                Q.p, Q.inv_p, ckq, QCx, QCy, QCz, ACQx, ACQy, ACQz, sm);
               P = Pn;
             }
           }
