@@ -1555,9 +1555,11 @@ void hfg_autotune_opts_default(hfg_autotune_opts* o) {
   o->n_prim = 3;
   o->max_energy_error = 5e-9;
   o->repeats = 2;
-  o->tiles[0] = 16;
-  o->tiles[1] = 256;
-  o->n_tile = 2;
+  o->tiles[0] = 8;
+  o->tiles[1] = 16;
+  o->tiles[2] = 32;
+  o->tiles[3] = 256;
+  o->n_tile = 4;
 }
 
 int hfg_jk_autotune(hfg_ctx* ctx, const hfg_jk_opts* base, int nspin, const double* dPt, const double* dPs,

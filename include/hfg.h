@@ -240,7 +240,7 @@ int hfg_jk_last_stats(const hfg_ctx* ctx, hfg_jk_stats* stats);
  * `found` is 0.  Then the best pair is timed with each quartet tile of
  * `tiles` (hfg_jk_opts.tile) and the fastest within the budget kept.  Empty
  * candidate lists use 1e-7, 1e-6, 1e-5, 1e-4 (FP32), 1e-15, 1e-14, 1e-13
- * (primitives) and tiles 16, 256 (beside the default 64); the default budget
+ * (primitives) and tiles 8, 16, 32, 256 (beside the default 64); the default budget
  * is 5e-9 Eh.
  */
 typedef struct {

@@ -160,12 +160,12 @@ def test_autotune_picks_fastest_within_energy_budget():
     dP = torch.from_numpy(np.ascontiguousarray(P)).to(torch.device("cuda", 0))
     torch.cuda.synchronize()  # the context runs on its own stream
     best, rep = ctx.autotune(dP.data_ptr(), dP.data_ptr(), max_energy_error=5e-9, repeats=1)
-    # 12 threshold pairs, then the library's two extra quartet tiles on the best pair
-    assert rep["found"] and len(rep["candidates"]) == 14
-    assert [c.get("tile") for c in rep["candidates"][12:]] == [16, 256]
+    # 12 threshold pairs, then the library's four extra quartet tiles on the best pair
+    assert rep["found"] and len(rep["candidates"]) == 16
+    assert [c.get("tile") for c in rep["candidates"][12:]] == [8, 16, 32, 256]
     ok = [c for c in rep["candidates"] if abs(c["energy_error"]) <= 5e-9]
     assert rep["best_ms"] == min(c["ms"] for c in ok)
-    assert best.tile in (0, 16, 256)
+    assert best.tile in (0, 8, 16, 32, 256)
     J0, K0 = ctx.jk(P, opts=JKOptions.make(prim=0.0))
     J1, K1 = ctx.jk(P, opts=best)
     dE = 0.5 * np.sum(P * (J1 - J0)) - 0.25 * np.sum(P * (K1[0] - K0[0]))
