@@ -187,10 +187,10 @@ template <int LA, int LB, int LC, int LD, typename T> struct MinBlocks {
 #ifdef HFG_JK_MIN_BLOCKS_F32
   static constexpr int f32 = HFG_JK_MIN_BLOCKS_F32;
 #else
-  static constexpr int f32 = (code == 0 || code == 1000 || code == 1010)   ? 4
-                             : (code == 1100 || code == 2000 || code == 2100) ? 3
-                             : (L >= 5 || code == 1111)                       ? 1
-                                                                              : 2;
+  static constexpr int f32 = (code == 0 || code == 1000 || code == 1010 || code == 1100 || code == 2000) ? 4
+                             : (code == 2100 || code == 1110 || code == 2010)                           ? 3
+                             : (L >= 5 || code == 1111)                                                 ? 1
+                                                                                                        : 2;
 #endif
   static constexpr int value = sizeof(T) == 4 ? f32 : f64;
 };
@@ -208,24 +208,25 @@ template <int LA, int LB, int LC, int LD, typename T> struct MinBlocks {
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 
-// K'[a,c], K'[b,c] of FP32 launches are summed over the lanes that share the
-// ket's first shell c before their atomics (kets are ordered by AO index
-// within each Schwarz bucket, so such lanes are neighbours).  FP64 launches
-// do the same for the classes where it measured faster ((10|10), (11|10),
-// (20|10): 4-12% each in an FP64 build of (H2O)64 cc-pVDZ) and add per lane
-// otherwise.  HFG_JK_SEG_F64=0/1 and HFG_JK_SEG_F32=0 override this in
-// tuning builds.
+// K'[a,c], K'[b,c] are summed over the lanes that share the ket's first
+// shell c before their atomics (kets are ordered by AO index within each
+// Schwarz bucket, so such lanes are neighbours) in the launches where that
+// measured faster on (H2O)64 cc-pVDZ: FP32 launches except (21|11), (21|20)
+// and (22|10), and the FP64 launches of (10|10), (11|10), (20|10) (4-12%
+// each).  The others add per lane.  HFG_JK_SEG_F64 / HFG_JK_SEG_F32 = 0 or 1
+// override this in tuning builds.
 #ifndef HFG_JK_SEG_F64
 #define HFG_JK_SEG_F64 -1
 #endif
 #ifndef HFG_JK_SEG_F32
-#define HFG_JK_SEG_F32 1
+#define HFG_JK_SEG_F32 -1
 #endif
 template <int LA, int LB, int LC, int LD, typename T> struct SegReduce {
   static constexpr int code = LA * 1000 + LB * 100 + LC * 10 + LD;
   static constexpr bool f64_table = code == 1010 || code == 1110 || code == 2010;
-  static constexpr bool value =
-      sizeof(T) == 4 ? HFG_JK_SEG_F32 != 0 : (HFG_JK_SEG_F64 < 0 ? f64_table : HFG_JK_SEG_F64 != 0);
+  static constexpr bool f32_table = !(code == 2111 || code == 2120 || code == 2210);
+  static constexpr bool value = sizeof(T) == 4 ? (HFG_JK_SEG_F32 < 0 ? f32_table : HFG_JK_SEG_F32 != 0)
+                                               : (HFG_JK_SEG_F64 < 0 ? f64_table : HFG_JK_SEG_F64 != 0);
 };
 
 // Sum of v over this lane's run of lanes [lane, end), left in the run's
