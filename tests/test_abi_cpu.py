@@ -1,6 +1,7 @@
 """CPU-side checks of the product: the C-ABI library loads and exports every
-entry point of include/hfg.h, and the host-side basis and cluster builders
-agree with the oracle's restatement of hf-rs's build_basis."""
+entry point of include/hfg.h, its option defaults are the documented ones,
+and the host-side basis and cluster builders agree with the oracle's
+restatement of hf-rs's build_basis."""
 import os
 import subprocess
 
@@ -51,3 +52,21 @@ def test_water_cluster_is_seeded_and_sane():
     pos = np.array([p for _, p in a])
     d = np.linalg.norm(pos[:, None] - pos[None], axis=-1) + np.eye(len(a)) * 1e9
     assert d.min() > 1.0  # bohr
+
+
+def test_default_options_are_the_documented_ones():
+    # the option defaults of include/hfg.h, read through the C ABI (host
+    # code only: no device is touched)
+    if not os.path.exists(hl.library_path()):
+        pytest.skip("libhfg.so not built")
+    import ctypes
+    L = hl.load_library()
+    j = hl.JKOptions()
+    L.hfg_jk_opts_default(ctypes.byref(j))
+    assert (j.schwarz_threshold, j.prim_threshold, j.precision, j.deterministic, j.tile) == (1e-12, 0.0, 0, 0, 0)
+    a = hl.AutotuneOptions()
+    L.hfg_autotune_opts_default(ctypes.byref(a))
+    assert list(a.fp32_thresholds[:a.n_fp32]) == [1e-7, 1e-6, 1e-5, 1e-4]
+    assert list(a.prim_thresholds[:a.n_prim]) == [1e-15, 1e-14, 1e-13]
+    assert list(a.tiles[:a.n_tile]) == [8, 16, 32, 256]
+    assert a.max_energy_error == 5e-9 and a.repeats == 2
